@@ -1,0 +1,165 @@
+/*
+ * nexd.h -- C-ABI of the B200 time-stepping library (libnexd.so).
+ *
+ * Drop-in boundary for NEXD-3D's solver time loop:
+ *   subroutine timeloop3D(par, myrank)   src/timeloopMod.f90:42-674
+ * called from program_solver.f90:71.  A Fortran host keeps readMesh /
+ * readSrc / readRec / prepareSources (src/meshMod.f90:1642-1658,
+ * src/sourceReceiverMod.f90:705-839) and the seismogram writers
+ * (src/timeloopMod.f90:591-656), fills one nexd_desc with plain pointers to
+ * the arrays it already holds, and calls the entry points below through
+ * ISO_C_BINDING instead of running the element loop itself.
+ *
+ * Conventions (all entry points):
+ *  - every function returns an int status, NEXD_OK (0) on success; no entry
+ *    point calls exit() or stop (the reference stops or MPI_Aborts,
+ *    src/mpiMod.f90:287-307);
+ *  - arrays are in Fortran (column-major) order with the shapes given in the
+ *    comments, integer indices are 1-based as in the reference databases;
+ *  - the caller owns every host array; nexd_create copies what it needs, so
+ *    the descriptor may be freed after it returns;
+ *  - the library owns device memory, one CUDA stream and its CUDA graphs;
+ *  - a context is not thread-safe: use one context per host thread.
+ */
+#ifndef NEXD_H
+#define NEXD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NEXD_ABI_VERSION 1
+
+enum nexd_status {
+  NEXD_OK = 0,
+  NEXD_ERR_INVALID = 1,     /* bad argument or inconsistent descriptor */
+  NEXD_ERR_CUDA = 2,        /* CUDA runtime error (message has the details) */
+  NEXD_ERR_NOMEM = 3,       /* device allocation failed */
+  NEXD_ERR_UNSUPPORTED = 4, /* valid but not supported by this build (e.g. order) */
+  NEXD_ERR_NONFINITE = 5,   /* NaN/Inf detected in the wavefield */
+  NEXD_ERR_NODEVICE = 6     /* no CUDA device visible */
+};
+
+/* Time integrators: 1..3 are the reference's `timeint` values
+ * (src/timeloopMod.f90:230-248, src/rungekuttaMod.f90:27-120); 4 is the
+ * Carpenter-Kennedy (1994) 2N-storage 5-stage 4th-order scheme. */
+enum nexd_timeint { NEXD_EULER = 1, NEXD_RK2 = 2, NEXD_RK3 = 3, NEXD_LSERK4 = 4 };
+
+/* Receiver trace components, in this order: plotu{x,y,z}, plotv{x,y,z},
+ * plota{x,y,z} of src/timeloopMod.f90:358-373. */
+#define NEXD_NCOMP 9
+
+typedef struct nexd_desc {
+  int32_t abi_version; /* NEXD_ABI_VERSION */
+  int32_t N;           /* polynomial order (ORDER, src/constants.h:26) */
+  int32_t Np;          /* (N+1)(N+2)(N+3)/6 */
+  int32_t NpF;         /* (N+1)(N+2)/2 */
+  int32_t nelem;       /* K, elements of the (single) partition */
+  int32_t nMB;         /* Zener mechanisms; 0 when attenuation is off */
+  int32_t attenuation; /* par%attenuation */
+  int32_t set_pml;     /* par%set_pml */
+  int32_t timeint;     /* enum nexd_timeint */
+  int32_t nt;          /* par%nt */
+  double dt;           /* deltat = dtfactor * cfl (src/timeloopMod.f90:199) */
+  double init_value;   /* start value of every field; the reference uses 1e-24 */
+
+  /* Reference-element operators, FP64 (mesh%Dr/Ds/Dt/lift/fmask). */
+  const double* Dr;      /* (Np,Np) */
+  const double* Ds;      /* (Np,Np) */
+  const double* Dt;      /* (Np,Np) */
+  const double* lift;    /* (Np,4*NpF) */
+  const double* invmass; /* (Np,Np) = V V^T (src/timeloopMod.f90:302) */
+  const int32_t* fmask;  /* (NpF,4), 1-based node ids */
+
+  /* Affine-element geometry, one value per element (the reference stores the
+   * same constant on every node: mesh%rx(ibool(1,ie)) etc.). */
+  const double* metric;      /* (9,K): rx ry rz sx sy sz tx ty tz */
+  const double* jacobian;    /* (K) */
+  const double* fscale;      /* (4,K): sJ/J of each face */
+  const double* nnormal;     /* (3,4,K) outward unit normal of each face */
+  const double* stangential; /* (3,4,K) */
+  const double* ttangential; /* (3,4,K) */
+
+  /* Material (unrelaxed values when attenuation is on). */
+  const double* rho;     /* (K) */
+  const double* vpu;     /* (K) */
+  const double* vsu;     /* (K) */
+  const double* lambdau; /* (K) */
+  const double* muu;     /* (K) */
+  const double* ylambda; /* (nMB,K) */
+  const double* ymu;     /* (nMB,K) */
+  const double* wl;      /* (nMB) relaxation frequencies */
+
+  /* Connectivity (single partition: mpi_* arrays are not needed). */
+  const int32_t* neighbor; /* (4,K), 0 on a domain boundary */
+  const int32_t* face;     /* (4,K): neighbour's face 1..4, -1 free, -2 absorbing */
+  const int32_t* ibn;      /* (NpF,4,K): neighbour's node id (global 1-based) matching
+                              face node i of this element (src/meshMod.f90:939-987) */
+
+  /* NPML (src/pmlMod.f90:90-165); ignored when set_pml == 0. */
+  const int32_t* pmlcheck;     /* (K) 0/1 */
+  const double* pml_profiles;  /* (K*Np,9): ddx ddy ddz alphax alphay alphaz kx ky kz */
+
+  /* Sources (srcVar after prepareSources). */
+  int32_t nsrc;
+  const int32_t* srcelem;       /* (nsrc) 1-based */
+  const int32_t* srctype;       /* (nsrc) 0 force, 1 moment tensor */
+  const double* srcInt;         /* (Np,nsrc) interpolation weights */
+  const double* srcangle_force; /* (3,nsrc) unit force direction */
+  const double* srcM;           /* (6,nsrc) Mxx Myy Mzz Mxy Mxz Myz */
+  int32_t stf_per_step;         /* 1: one value per step (reference); else one value per RK stage */
+  const double* stf;            /* (stf_per_step,nt,nsrc): plotstf(:,2,:) as used in the source term */
+
+  /* Receivers (recVar). */
+  int32_t nrec;
+  const int32_t* recelem; /* (nrec) 1-based */
+  const double* recInt;   /* (Np,nrec) */
+
+  /* Batched independent wavefields sharing this mesh (1 = one simulation).
+   * Source i acts on wavefield srcbatch[i]; every wavefield records every
+   * receiver. */
+  int32_t nbatch;
+  const int32_t* srcbatch; /* (nsrc) 0-based wavefield index, may be NULL when nbatch == 1 */
+} nexd_desc;
+
+typedef struct nexd_ctx nexd_ctx;
+
+/* Builds device state from the descriptor (replaces the set-up part of
+ * timeloop3D, src/timeloopMod.f90:162-356). */
+int nexd_create(const nexd_desc* desc, nexd_ctx** out);
+
+/* Advances time steps it_begin..it_end (1-based, inclusive), recording the
+ * receiver traces of each step before its update, as the hot loop
+ * src/timeloopMod.f90:357-589 does. */
+int nexd_run(nexd_ctx* ctx, int32_t it_begin, int32_t it_end);
+
+/* Copies receiver traces to `out`, shape (nrec, nt, 9, nbatch), for the steps
+ * run so far (other steps hold 0). */
+int nexd_get_traces(nexd_ctx* ctx, float* out);
+
+/* Copies the velocity-stress wavefield of batch member `b` to `out`, shape
+ * (K*Np, 9), the layout of q in src/timeloopMod.f90:107. */
+int nexd_get_field(nexd_ctx* ctx, int32_t b, float* out);
+
+/* Overwrites the wavefield of batch member `b` from `in`, shape (K*Np, 9). */
+int nexd_set_field(nexd_ctx* ctx, int32_t b, const float* in);
+
+/* Last error message of ctx (or of the last failed nexd_create when ctx is
+ * NULL), NUL-terminated and truncated to len bytes. */
+int nexd_last_error(const nexd_ctx* ctx, char* buf, size_t len);
+
+/* Number of kernel launches issued by nexd_run so far (for launch-count
+ * reporting). */
+int nexd_launch_count(const nexd_ctx* ctx, int64_t* out);
+
+/* Frees device memory, the stream and graphs of ctx. */
+int nexd_destroy(nexd_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEXD_H */

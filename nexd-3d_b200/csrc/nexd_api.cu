@@ -1,0 +1,659 @@
+// C-ABI of libnexd.so (include/nexd.h): device set-up and the time loop.
+//
+// Replaces timeloop3D (src/timeloopMod.f90:42-674) for a single partition.
+// Host work here is set-up only (FP64 -> FP32 element records, connectivity
+// patterns, source patterns); every time step runs on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/nexd.h"
+#include "stage_kernel.cuh"
+
+using namespace nexd_dev;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+// Carpenter & Kennedy (1994) 5-stage, 4th-order, 2N-storage coefficients.
+const double kRK4A[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                         -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double kRK4B[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                         1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                         2277821191437.0 / 14882151754819.0};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct nexd_ctx {
+  std::string err;
+  int N = 0, Np = 0, NpF = 0, K = 0, nMB = 0, nt = 0, nstage = 1, timeint = 4, nbatch = 1;
+  int Kpml = 0;  // PML elements occupy internal indices [0, Kpml)
+  bool att = false, pml = false;
+  double dt = 0.0;
+  long long ldq = 0, ldt = 0, lda = 0;
+  int nrec = 0, nslot = 0, nsrc = 0, nspt = 1;
+  std::vector<int> new2old, old2new;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int nsm = 148;
+  int grid_pml = 0, grid_main = 0;
+  size_t smem_pml = 0, smem_main = 0;
+  // device arrays
+  float *D = nullptr, *L = nullptr, *geo = nullptr, *ael = nullptr, *wl = nullptr, *prof = nullptr;
+  int4 *nbr = nullptr, *fcode = nullptr;
+  unsigned char* patterns = nullptr;
+  float* qbuf[3] = {nullptr, nullptr, nullptr};
+  float* res = nullptr;
+  float *th = nullptr, *th2 = nullptr, *aux = nullptr, *aux2 = nullptr;
+  int *src_head = nullptr, *src_next = nullptr, *src_batch = nullptr;
+  float *src_pat = nullptr, *stf = nullptr;
+  int *rec_slot = nullptr, *recelem = nullptr, *recslot_of_rec = nullptr;
+  float *recInt = nullptr, *abuf = nullptr, *u = nullptr, *traces = nullptr;
+  int* flag = nullptr;
+  int cur = 0;  // index of the buffer holding the current wavefield
+  int64_t launches = 0;
+  std::vector<void*> allocations;
+};
+
+namespace {
+
+int set_err(nexd_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m; else g_create_error = m;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                  \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return set_err(ctx, e_ == cudaErrorMemoryAllocation ? NEXD_ERR_NOMEM : NEXD_ERR_CUDA,  \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+  } while (0)
+
+template <class T>
+int dalloc(nexd_ctx* c, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  void* v = nullptr;
+  cudaError_t e = cudaMalloc(&v, count * sizeof(T));
+  if (e != cudaSuccess)
+    return set_err(c, e == cudaErrorMemoryAllocation ? NEXD_ERR_NOMEM : NEXD_ERR_CUDA,
+                   std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  c->allocations.push_back(v);
+  *p = static_cast<T*>(v);
+  return NEXD_OK;
+}
+
+template <class T>
+int upload(nexd_ctx* c, T** p, const std::vector<T>& h) {
+  int st = dalloc(c, p, h.size());
+  if (st) return st;
+  if (!h.empty()) CUDA_TRY(c, cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return NEXD_OK;
+}
+
+int fill(nexd_ctx* c, float* p, size_t n, float v) {
+  std::vector<float> h(std::min<size_t>(n, size_t(1) << 24), v);
+  for (size_t off = 0; off < n; off += h.size()) {
+    const size_t m = std::min(h.size(), n - off);
+    CUDA_TRY(c, cudaMemcpy(p + off, h.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return NEXD_OK;
+}
+
+template <int N>
+size_t smem_bytes(bool pml) {
+  using O = Order<N>;
+  size_t f = 3 * O::Np * O::Np + O::NF * O::Np + O::E * GEO_STRIDE + O::E * O::Np * O::QS + O::E * O::NF * 4 +
+             O::E * 4 * O::GS;
+  if (pml) f += O::E * O::Np * O::CS;
+  return f * sizeof(float);
+}
+
+using KernelFn = void (*)(const StageArgs);
+
+template <int N>
+KernelFn pick(bool att, bool pml, int mode) {
+  if (mode == MODE_LSERK) {
+    if (att) return pml ? stage_kernel<N, true, true, MODE_LSERK> : stage_kernel<N, true, false, MODE_LSERK>;
+    return pml ? stage_kernel<N, false, true, MODE_LSERK> : stage_kernel<N, false, false, MODE_LSERK>;
+  }
+  if (att) return pml ? stage_kernel<N, true, true, MODE_TVD> : stage_kernel<N, true, false, MODE_TVD>;
+  return pml ? stage_kernel<N, false, true, MODE_TVD> : stage_kernel<N, false, false, MODE_TVD>;
+}
+
+KernelFn pick_kernel(int N, bool att, bool pml, int mode, size_t& smem) {
+  switch (N) {
+    case 1: smem = smem_bytes<1>(pml); return pick<1>(att, pml, mode);
+    case 2: smem = smem_bytes<2>(pml); return pick<2>(att, pml, mode);
+    case 3: smem = smem_bytes<3>(pml); return pick<3>(att, pml, mode);
+    case 4: smem = smem_bytes<4>(pml); return pick<4>(att, pml, mode);
+    case 5: smem = smem_bytes<5>(pml); return pick<5>(att, pml, mode);
+    default: smem = 0; return nullptr;
+  }
+}
+
+int elements_per_chunk(int N) {
+  const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
+  return 256 / Np;
+}
+
+int validate(const nexd_desc* d) {
+  if (!d) return set_err(nullptr, NEXD_ERR_INVALID, "null descriptor");
+  if (d->abi_version != NEXD_ABI_VERSION) return set_err(nullptr, NEXD_ERR_INVALID, "ABI version mismatch");
+  if (d->N < 1 || d->N > 5)
+    return set_err(nullptr, NEXD_ERR_UNSUPPORTED, "polynomial order must be 1..5 in this build");
+  const int Np = (d->N + 1) * (d->N + 2) * (d->N + 3) / 6, NpF = (d->N + 1) * (d->N + 2) / 2;
+  if (d->Np != Np || d->NpF != NpF) return set_err(nullptr, NEXD_ERR_INVALID, "Np/NpF inconsistent with N");
+  if (d->nelem <= 0) return set_err(nullptr, NEXD_ERR_INVALID, "nelem must be positive");
+  if (d->nt <= 0) return set_err(nullptr, NEXD_ERR_INVALID, "nt must be positive");
+  if (!(d->dt > 0.0) || !std::isfinite(d->dt)) return set_err(nullptr, NEXD_ERR_INVALID, "dt must be positive");
+  if (d->timeint < 1 || d->timeint > 4) return set_err(nullptr, NEXD_ERR_INVALID, "timeint must be 1..4");
+  if (d->nbatch < 1) return set_err(nullptr, NEXD_ERR_INVALID, "nbatch must be >= 1");
+  if (d->attenuation && (d->nMB < 1 || d->nMB > 8 || !d->wl || !d->ylambda || !d->ymu))
+    return set_err(nullptr, NEXD_ERR_INVALID, "attenuation needs 1..8 mechanisms with wl/ylambda/ymu");
+  if (d->set_pml && (!d->pmlcheck || !d->pml_profiles))
+    return set_err(nullptr, NEXD_ERR_INVALID, "set_pml needs pmlcheck and pml_profiles");
+  const void* req[] = {d->Dr, d->Ds, d->Dt, d->lift, d->fmask, d->metric, d->jacobian, d->fscale, d->nnormal,
+                       d->stangential, d->ttangential, d->rho, d->vpu, d->vsu, d->lambdau, d->muu, d->neighbor,
+                       d->face, d->ibn};
+  for (const void* p : req)
+    if (!p) return set_err(nullptr, NEXD_ERR_INVALID, "descriptor has a null array");
+  if (d->nsrc < 0 || d->nrec < 0) return set_err(nullptr, NEXD_ERR_INVALID, "negative source/receiver count");
+  if (d->nsrc > 0 && (!d->srcelem || !d->srctype || !d->srcInt || !d->stf || !d->invmass || d->stf_per_step < 1))
+    return set_err(nullptr, NEXD_ERR_INVALID, "sources need srcelem/srctype/srcInt/stf/invmass");
+  if (d->nrec > 0 && (!d->recelem || !d->recInt)) return set_err(nullptr, NEXD_ERR_INVALID, "receivers need recelem/recInt");
+  for (int i = 0; i < d->nsrc; ++i) {
+    if (d->srcelem[i] < 1 || d->srcelem[i] > d->nelem) return set_err(nullptr, NEXD_ERR_INVALID, "srcelem out of range");
+    if (d->srctype[i] != 0 && d->srctype[i] != 1) return set_err(nullptr, NEXD_ERR_INVALID, "srctype must be 0 or 1");
+    if (d->srctype[i] == 0 && !d->srcangle_force) return set_err(nullptr, NEXD_ERR_INVALID, "force source without direction");
+    if (d->srctype[i] == 1 && !d->srcM) return set_err(nullptr, NEXD_ERR_INVALID, "moment source without tensor");
+    if (d->nbatch > 1 && d->srcbatch && (d->srcbatch[i] < 0 || d->srcbatch[i] >= d->nbatch))
+      return set_err(nullptr, NEXD_ERR_INVALID, "srcbatch out of range");
+  }
+  for (int i = 0; i < d->nrec; ++i)
+    if (d->recelem[i] < 1 || d->recelem[i] > d->nelem) return set_err(nullptr, NEXD_ERR_INVALID, "recelem out of range");
+  for (int e = 0; e < d->nelem; ++e) {
+    for (int f = 0; f < 4; ++f) {
+      const int nb = d->neighbor[4 * e + f], fc = d->face[4 * e + f];
+      if (nb < 0 || nb > d->nelem) return set_err(nullptr, NEXD_ERR_INVALID, "neighbor index out of range");
+      if (nb == 0 && fc != -1 && fc != -2)
+        return set_err(nullptr, NEXD_ERR_INVALID, "boundary face that is neither free (-1) nor absorbing (-2)");
+      if (nb > 0 && (fc < 1 || fc > 4)) return set_err(nullptr, NEXD_ERR_INVALID, "interior face without neighbour face id");
+    }
+    if (!(std::fabs(d->jacobian[e]) > 0.0)) return set_err(nullptr, NEXD_ERR_INVALID, "zero Jacobian");
+    if (!(d->rho[e] > 0.0) || !(d->vpu[e] > 0.0) || !(d->vsu[e] > 0.0))
+      return set_err(nullptr, NEXD_ERR_INVALID, "non-positive material value");
+  }
+  return NEXD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nexd_create(const nexd_desc* d, nexd_ctx** out) {
+  if (!out) return set_err(nullptr, NEXD_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  int st = validate(d);
+  if (st) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_err(nullptr, NEXD_ERR_NODEVICE, "no CUDA device visible");
+  }
+  nexd_ctx* c = new nexd_ctx;
+  auto fail = [&](int code) {
+    g_create_error = c->err;
+    nexd_destroy(c);
+    return code;
+  };
+  const int N = d->N, Np = d->Np, NpF = d->NpF, K = d->nelem, NF = 4 * NpF;
+  c->N = N; c->Np = Np; c->NpF = NpF; c->K = K;
+  c->att = d->attenuation != 0;
+  c->pml = d->set_pml != 0;
+  c->nMB = c->att ? d->nMB : 0;
+  c->nt = d->nt;
+  c->timeint = d->timeint;
+  c->nstage = d->timeint == 4 ? 5 : (d->timeint == 3 ? 3 : (d->timeint == 2 ? 2 : 1));
+  c->nbatch = d->nbatch;
+  c->dt = d->dt;
+  c->nsrc = d->nsrc;
+  c->nrec = d->nrec;
+  c->nspt = d->stf_per_step;
+  if (cudaGetDevice(&c->device) != cudaSuccess) return fail(set_err(c, NEXD_ERR_CUDA, "cudaGetDevice failed"));
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(set_err(c, NEXD_ERR_CUDA, "cudaStreamCreate failed"));
+
+  // ---- internal element order: PML elements first, each group in mesh order ----
+  c->new2old.reserve(K);
+  if (c->pml)
+    for (int e = 0; e < K; ++e)
+      if (d->pmlcheck[e]) c->new2old.push_back(e);
+  c->Kpml = int(c->new2old.size());
+  for (int e = 0; e < K; ++e)
+    if (!(c->pml && d->pmlcheck[e])) c->new2old.push_back(e);
+  c->old2new.assign(K, 0);
+  for (int i = 0; i < K; ++i) c->old2new[c->new2old[i]] = i;
+
+  // ---- face patterns: rows 0..3 own face masks, then neighbour maps ----
+  std::vector<unsigned char> pat(size_t(4) * NpF);
+  for (int f = 0; f < 4; ++f)
+    for (int i = 0; i < NpF; ++i) pat[size_t(f) * NpF + i] = (unsigned char)(d->fmask[f * NpF + i] - 1);
+  std::map<std::vector<unsigned char>, int> patid;
+  std::vector<int> h_nbr(size_t(K) * 4, -1), h_fcode(size_t(K) * 4, -2);
+  for (int ni = 0; ni < K; ++ni) {
+    const int e = c->new2old[ni];
+    for (int f = 0; f < 4; ++f) {
+      const int nb = d->neighbor[4 * e + f];
+      if (nb == 0) {
+        h_fcode[4 * ni + f] = d->face[4 * e + f];  // -1 free, -2 absorbing
+        continue;
+      }
+      std::vector<unsigned char> row(NpF);
+      for (int i = 0; i < NpF; ++i) {
+        const long long gn = (long long)d->ibn[(size_t(e) * 4 + f) * NpF + i] - 1 - (long long)(nb - 1) * Np;
+        if (gn < 0 || gn >= Np) return fail(set_err(c, NEXD_ERR_INVALID, "ibn does not point into the neighbour element"));
+        row[i] = (unsigned char)gn;
+      }
+      auto it = patid.find(row);
+      int id;
+      if (it == patid.end()) {
+        id = 4 + int(patid.size());
+        patid[row] = id;
+        pat.insert(pat.end(), row.begin(), row.end());
+      } else {
+        id = it->second;
+      }
+      h_nbr[4 * ni + f] = c->old2new[nb - 1];
+      h_fcode[4 * ni + f] = id;
+    }
+  }
+  if (patid.size() > 250) return fail(set_err(c, NEXD_ERR_UNSUPPORTED, "too many distinct face permutations"));
+
+  // ---- element records ----
+  std::vector<float> h_geo(size_t(K) * GEO_STRIDE, 0.f);
+  for (int ni = 0; ni < K; ++ni) {
+    const int e = c->new2old[ni];
+    float* g = &h_geo[size_t(ni) * GEO_STRIDE];
+    for (int i = 0; i < 9; ++i) g[G_RX + i] = float(d->metric[9 * e + i]);
+    for (int f = 0; f < 4; ++f) {
+      g[G_FS + f] = float(0.5 * d->fscale[4 * e + f]);
+      for (int k = 0; k < 3; ++k) {
+        g[G_N + 3 * f + k] = float(d->nnormal[(size_t(e) * 4 + f) * 3 + k]);
+        g[G_S + 3 * f + k] = float(d->stangential[(size_t(e) * 4 + f) * 3 + k]);
+        g[G_T + 3 * f + k] = float(d->ttangential[(size_t(e) * 4 + f) * 3 + k]);
+      }
+    }
+    const double lam = d->lambdau[e], mu = d->muu[e], rho = d->rho[e], vp = d->vpu[e], vs = d->vsu[e];
+    g[G_E1] = float(-(lam + 2 * mu));
+    g[G_E2] = float(-lam);
+    g[G_E3] = float(-mu);
+    g[G_E4] = float(-1.0 / rho);
+    g[G_VP] = float(vp);
+    g[G_VS] = float(vs);
+    g[G_L2M] = float(lam + 2 * mu);
+    g[G_MU] = float(mu);
+    g[G_LAM] = float(lam);
+    g[G_IRHO] = float(1.0 / rho);
+    g[G_C] = float(lam / (lam + 2 * mu));
+    g[G_IZP] = float(1.0 / (rho * vp));
+    g[G_IZS] = float(1.0 / (rho * vs));
+    g[G_AP] = float(1.0 / (lam + 2 * mu));
+    g[G_AS] = float(1.0 / (2 * mu));
+  }
+  std::vector<float> h_D(size_t(3) * Np * Np), h_L(size_t(NF) * Np);
+  for (int k = 0; k < Np; ++k)
+    for (int n = 0; n < Np; ++n) {
+      h_D[size_t(k) * Np + n] = float(d->Dr[size_t(k) * Np + n]);
+      h_D[size_t(Np) * Np + size_t(k) * Np + n] = float(d->Ds[size_t(k) * Np + n]);
+      h_D[size_t(2) * Np * Np + size_t(k) * Np + n] = float(d->Dt[size_t(k) * Np + n]);
+    }
+  for (int j = 0; j < NF; ++j)
+    for (int n = 0; n < Np; ++n) h_L[size_t(j) * Np + n] = float(d->lift[size_t(j) * Np + n]);
+  std::vector<float> h_ael, h_wl;
+  if (c->att) {
+    h_ael.assign(size_t(K) * 3 * c->nMB, 0.f);
+    for (int ni = 0; ni < K; ++ni) {
+      const int e = c->new2old[ni];
+      for (int l = 0; l < c->nMB; ++l) {
+        const double a1 = -d->lambdau[e] * d->ylambda[size_t(e) * c->nMB + l];
+        const double a2 = -2.0 * d->muu[e] * d->ymu[size_t(e) * c->nMB + l];
+        h_ael[(size_t(ni) * c->nMB + l) * 3 + 0] = float(a1);
+        h_ael[(size_t(ni) * c->nMB + l) * 3 + 1] = float(a2);
+        h_ael[(size_t(ni) * c->nMB + l) * 3 + 2] = float(a1 + a2);
+      }
+    }
+    for (int l = 0; l < c->nMB; ++l) h_wl.push_back(float(d->wl[l]));
+  }
+  std::vector<float> h_prof;
+  if (c->pml && c->Kpml > 0) {
+    h_prof.assign(size_t(c->Kpml) * 9 * Np, 0.f);
+    const size_t ng = size_t(K) * Np;
+    for (int ni = 0; ni < c->Kpml; ++ni) {
+      const int e = c->new2old[ni];
+      for (int p = 0; p < 9; ++p)
+        for (int n = 0; n < Np; ++n)
+          h_prof[(size_t(ni) * 9 + p) * Np + n] = float(d->pml_profiles[p * ng + size_t(e) * Np + n]);
+    }
+  }
+
+  // ---- sources: per-element lists and FP64-built patterns ----
+  std::vector<int> h_head(K, -1), h_next(std::max(1, c->nsrc), -1), h_sb(std::max(1, c->nsrc), 0);
+  std::vector<float> h_spat(size_t(std::max(1, c->nsrc)) * 9 * Np, 0.f);
+  for (int i = c->nsrc - 1; i >= 0; --i) {
+    const int e = d->srcelem[i] - 1, ni = c->old2new[e];
+    h_next[i] = h_head[ni];
+    h_head[ni] = i;
+    h_sb[i] = (d->nbatch > 1 && d->srcbatch) ? d->srcbatch[i] : 0;
+    // invmass * (srcInt * a) / J [/ rho]  (src/timeloopMod.f90:327-356)
+    double amp[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (d->srctype[i] == 0) {
+      for (int k = 0; k < 3; ++k) amp[6 + k] = d->srcangle_force[3 * i + k] / d->rho[e];
+    } else {
+      const double* M = &d->srcM[6 * i];  // Mxx Myy Mzz Mxy Mxz Myz -> fields xx yy zz xy yz xz
+      amp[0] = M[0]; amp[1] = M[1]; amp[2] = M[2]; amp[3] = M[3]; amp[4] = M[5]; amp[5] = M[4];
+    }
+    for (int f = 0; f < 9; ++f) {
+      if (amp[f] == 0.0) continue;
+      for (int n = 0; n < Np; ++n) {
+        double acc = 0.0;
+        for (int k = 0; k < Np; ++k) acc += d->invmass[size_t(k) * Np + n] * d->srcInt[size_t(i) * Np + k] * amp[f];
+        h_spat[(size_t(i) * 9 + f) * Np + n] = float(acc / d->jacobian[e]);
+      }
+    }
+  }
+  std::vector<float> h_stf(size_t(std::max(1, c->nsrc)) * c->nt * c->nspt, 0.f);
+  for (size_t i = 0; i < size_t(c->nsrc) * c->nt * c->nspt; ++i) h_stf[i] = float(d->stf[i]);
+
+  // ---- receivers ----
+  std::vector<int> h_recslot_el(K, -1), h_recelem(std::max(1, c->nrec), 0), h_recslot(std::max(1, c->nrec), 0);
+  std::vector<float> h_recInt(size_t(std::max(1, c->nrec)) * Np, 0.f);
+  for (int r = 0; r < c->nrec; ++r) {
+    const int ni = c->old2new[d->recelem[r] - 1];
+    if (h_recslot_el[ni] < 0) h_recslot_el[ni] = c->nslot++;
+    h_recelem[r] = ni;
+    h_recslot[r] = h_recslot_el[ni];
+    for (int n = 0; n < Np; ++n) h_recInt[size_t(r) * Np + n] = float(d->recInt[size_t(r) * Np + n]);
+  }
+
+  // ---- device memory ----
+  const long long nodes = (long long)K * Np;
+  c->ldq = (nodes + 63) / 64 * 64;
+  c->ldt = c->ldq;
+  c->lda = ((long long)c->Kpml * Np + 63) / 64 * 64;
+  const int nb = c->nbatch;
+  if ((st = upload(c, &c->D, h_D)) || (st = upload(c, &c->L, h_L)) || (st = upload(c, &c->geo, h_geo)) ||
+      (st = upload(c, &c->patterns, pat)))
+    return fail(st);
+  {
+    std::vector<int4> nb4(K), fc4(K);
+    for (int i = 0; i < K; ++i) {
+      nb4[i] = make_int4(h_nbr[4 * i], h_nbr[4 * i + 1], h_nbr[4 * i + 2], h_nbr[4 * i + 3]);
+      fc4[i] = make_int4(h_fcode[4 * i], h_fcode[4 * i + 1], h_fcode[4 * i + 2], h_fcode[4 * i + 3]);
+    }
+    if ((st = upload(c, &c->nbr, nb4)) || (st = upload(c, &c->fcode, fc4))) return fail(st);
+  }
+  const int nq = (c->timeint == 3) ? 3 : 2;
+  for (int i = 0; i < nq; ++i) {
+    if ((st = dalloc(c, &c->qbuf[i], size_t(nb) * 9 * c->ldq))) return fail(st);
+    if ((st = fill(c, c->qbuf[i], size_t(nb) * 9 * c->ldq, float(d->init_value)))) return fail(st);
+  }
+  if (c->timeint == 4) {
+    if ((st = dalloc(c, &c->res, size_t(nb) * 9 * c->ldq))) return fail(st);
+    CUDA_TRY(c, cudaMemset(c->res, 0, size_t(nb) * 9 * c->ldq * sizeof(float)));
+  }
+  if (c->att) {
+    const size_t n = size_t(nb) * 6 * c->nMB * c->ldt;
+    if ((st = dalloc(c, &c->th, n)) || (st = dalloc(c, &c->th2, n))) return fail(st);
+    if ((st = fill(c, c->th, n, float(d->init_value)))) return fail(st);
+    CUDA_TRY(c, cudaMemset(c->th2, 0, n * sizeof(float)));
+    if ((st = upload(c, &c->ael, h_ael)) || (st = upload(c, &c->wl, h_wl))) return fail(st);
+  }
+  if (c->pml && c->Kpml > 0) {
+    const size_t n = size_t(nb) * 27 * c->lda;
+    if ((st = dalloc(c, &c->aux, n)) || (st = dalloc(c, &c->aux2, n))) return fail(st);
+    CUDA_TRY(c, cudaMemset(c->aux, 0, n * sizeof(float)));
+    CUDA_TRY(c, cudaMemset(c->aux2, 0, n * sizeof(float)));
+    if ((st = upload(c, &c->prof, h_prof))) return fail(st);
+  }
+  if ((st = upload(c, &c->src_head, h_head)) || (st = upload(c, &c->src_next, h_next)) ||
+      (st = upload(c, &c->src_batch, h_sb)) || (st = upload(c, &c->src_pat, h_spat)) || (st = upload(c, &c->stf, h_stf)))
+    return fail(st);
+  if ((st = upload(c, &c->rec_slot, h_recslot_el)) || (st = upload(c, &c->recelem, h_recelem)) ||
+      (st = upload(c, &c->recslot_of_rec, h_recslot)) || (st = upload(c, &c->recInt, h_recInt)))
+    return fail(st);
+  {
+    const size_t na = size_t(nb) * std::max(1, c->nslot) * 3 * Np;
+    if ((st = dalloc(c, &c->abuf, na)) || (st = fill(c, c->abuf, na, float(d->init_value)))) return fail(st);
+    // u accumulators start at the interpolated start value sum_j recInt(j) * init
+    std::vector<float> h_u(size_t(nb) * std::max(1, c->nrec) * 3, 0.f);
+    for (int b = 0; b < nb; ++b)
+      for (int r = 0; r < c->nrec; ++r) {
+        double s = 0.0;
+        for (int n = 0; n < Np; ++n) s += float(d->recInt[size_t(r) * Np + n]) * float(d->init_value);
+        for (int k = 0; k < 3; ++k) h_u[(size_t(b) * c->nrec + r) * 3 + k] = float(s);
+      }
+    if ((st = upload(c, &c->u, h_u))) return fail(st);
+    const size_t nt_ = size_t(nb) * std::max(1, c->nrec) * c->nt * 9;
+    if ((st = dalloc(c, &c->traces, nt_))) return fail(st);
+    CUDA_TRY(c, cudaMemset(c->traces, 0, nt_ * sizeof(float)));
+    if ((st = dalloc(c, &c->flag, 1))) return fail(st);
+    CUDA_TRY(c, cudaMemset(c->flag, 0, sizeof(int)));
+  }
+  // ---- launch configuration ----
+  const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
+  for (int which = 0; which < 2; ++which) {
+    const bool pmlk = which == 0;
+    size_t smem = 0;
+    KernelFn fn = pick_kernel(N, c->att, pmlk, mode, smem);
+    if (!fn) return fail(set_err(c, NEXD_ERR_UNSUPPORTED, "no kernel for this order"));
+    CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
+    if (per_sm < 1) return fail(set_err(c, NEXD_ERR_UNSUPPORTED, "stage kernel does not fit on an SM"));
+    const int nel = pmlk ? c->Kpml : K - c->Kpml;
+    const int E = elements_per_chunk(N);
+    const long long work = (long long)((nel + E - 1) / E) * nb;
+    const int grid = int(std::max<long long>(1, std::min<long long>(work, (long long)per_sm * c->nsm)));
+    if (pmlk) { c->grid_pml = grid; c->smem_pml = smem; }
+    else { c->grid_main = grid; c->smem_main = smem; }
+  }
+  CUDA_TRY(c, cudaDeviceSynchronize());
+  *out = c;
+  return NEXD_OK;
+}
+
+int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (it_begin < 1 || it_end > c->nt || it_begin > it_end) return set_err(c, NEXD_ERR_INVALID, "step range out of 1..nt");
+  const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
+  size_t smem_p = 0, smem_m = 0;
+  KernelFn kp = pick_kernel(c->N, c->att, true, mode, smem_p);
+  KernelFn km = pick_kernel(c->N, c->att, false, mode, smem_m);
+  StageArgs a{};
+  a.nbatch = c->nbatch;
+  a.nMB = c->nMB;
+  a.ldq = c->ldq;
+  a.ldt = c->ldt;
+  a.lda = c->lda;
+  a.D = c->D;
+  a.L = c->L;
+  a.geo = c->geo;
+  a.nbr = c->nbr;
+  a.fcode = c->fcode;
+  a.patterns = c->patterns;
+  a.ael = c->ael;
+  a.wl = c->wl;
+  a.prof = c->prof;
+  a.res = c->res;
+  a.th = c->th;
+  a.th2 = c->th2;
+  a.aux = c->aux;
+  a.aux2 = c->aux2;
+  a.dt = float(c->dt);
+  a.src_head = c->src_head;
+  a.src_next = c->src_next;
+  a.src_batch = c->src_batch;
+  a.src_pat = c->src_pat;
+  a.stf = c->stf;
+  a.nt = c->nt;
+  a.nspt = c->nspt;
+  a.rec_slot = c->rec_slot;
+  a.abuf = c->abuf;
+  a.nslot = std::max(1, c->nslot);
+  RecordArgs r{};
+  r.nrec = c->nrec;
+  r.nbatch = c->nbatch;
+  r.Np = c->Np;
+  r.nt = c->nt;
+  r.ldq = c->ldq;
+  r.recelem = c->recelem;
+  r.recslot = c->recslot_of_rec;
+  r.recInt = c->recInt;
+  r.abuf = c->abuf;
+  r.nslot = std::max(1, c->nslot);
+  r.u = c->u;
+  r.traces = c->traces;
+  r.dt = float(c->dt);
+  r.flag = c->flag;
+  const int rec_warps = c->nrec * c->nbatch;
+  for (int it = it_begin; it <= it_end; ++it) {
+    if (rec_warps > 0) {
+      r.it = it;
+      r.q = c->qbuf[c->cur];
+      const int threads = 128;
+      const int blocks = (rec_warps * 32 + threads - 1) / threads;
+      record_kernel<<<blocks, threads, 0, c->stream>>>(r);
+      ++c->launches;
+    }
+    a.it = it;
+    for (int s = 0; s < c->nstage; ++s) {
+      a.stage = s;
+      a.last_stage = (s == c->nstage - 1);
+      a.stage_first = (s == 0);
+      int in = c->cur, outb;
+      const float* qn = nullptr;
+      if (c->timeint == 4) {
+        a.ca = float(kRK4A[s]);
+        a.cb = float(kRK4B[s]);
+        outb = 1 - c->cur;
+      } else if (c->timeint == 1) {
+        a.ca = 0.f; a.cb = 1.f;
+        outb = 1 - c->cur;
+      } else if (c->timeint == 2) {
+        // stage 1: A -> B; stage 2: (A, B) -> A  (src/rungekuttaMod.f90:90-103)
+        if (s == 0) { a.ca = 0.f; a.cb = 1.f; in = c->cur; outb = 1 - c->cur; }
+        else { a.ca = 0.5f; a.cb = 0.5f; in = 1 - c->cur; outb = c->cur; qn = c->qbuf[c->cur]; }
+      } else {
+        // RK3: A -> B; (A,B) -> C; (A,C) -> A  (src/rungekuttaMod.f90:105-120)
+        const int A = c->cur, B = (c->cur + 1) % 3, C = (c->cur + 2) % 3;
+        if (s == 0) { a.ca = 0.f; a.cb = 1.f; in = A; outb = B; }
+        else if (s == 1) { a.ca = 0.75f; a.cb = 0.25f; in = B; outb = C; qn = c->qbuf[A]; }
+        else { a.ca = float(1.0 / 3.0); a.cb = float(2.0 / 3.0); in = C; outb = A; qn = c->qbuf[A]; }
+      }
+      a.q_in = c->qbuf[in];
+      a.q_out = c->qbuf[outb];
+      a.q_n = qn;
+      if (c->Kpml > 0) {
+        a.e_begin = 0;
+        a.e_end = c->Kpml;
+        kp<<<c->grid_pml, 256, c->smem_pml, c->stream>>>(a);
+        ++c->launches;
+      }
+      if (c->K > c->Kpml) {
+        a.e_begin = c->Kpml;
+        a.e_end = c->K;
+        km<<<c->grid_main, 256, c->smem_main, c->stream>>>(a);
+        ++c->launches;
+      }
+      if (c->timeint == 4 || c->timeint == 1) c->cur = outb;
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  int flag = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (flag) return set_err(c, NEXD_ERR_NONFINITE, "non-finite value in the wavefield at a receiver");
+  return NEXD_OK;
+}
+
+int nexd_get_traces(nexd_ctx* c, float* out) {
+  if (!c || !out) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  const size_t n = size_t(c->nbatch) * c->nrec * c->nt * 9;
+  if (n == 0) return NEXD_OK;
+  CUDA_TRY(c, cudaMemcpyAsync(out, c->traces, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return NEXD_OK;
+}
+
+int nexd_get_field(nexd_ctx* c, int32_t b, float* out) {
+  if (!c || !out) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  if (b < 0 || b >= c->nbatch) return set_err(c, NEXD_ERR_INVALID, "batch index out of range");
+  const size_t nodes = size_t(c->K) * c->Np;
+  std::vector<float> h(size_t(9) * c->ldq);
+  CUDA_TRY(c, cudaMemcpyAsync(h.data(), c->qbuf[c->cur] + size_t(b) * 9 * c->ldq, h.size() * sizeof(float),
+                              cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  for (int f = 0; f < 9; ++f)
+    for (int ni = 0; ni < c->K; ++ni) {
+      const int e = c->new2old[ni];
+      std::memcpy(out + f * nodes + size_t(e) * c->Np, h.data() + f * c->ldq + size_t(ni) * c->Np, c->Np * sizeof(float));
+    }
+  return NEXD_OK;
+}
+
+int nexd_set_field(nexd_ctx* c, int32_t b, const float* in) {
+  if (!c || !in) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  if (b < 0 || b >= c->nbatch) return set_err(c, NEXD_ERR_INVALID, "batch index out of range");
+  const size_t nodes = size_t(c->K) * c->Np;
+  std::vector<float> h(size_t(9) * c->ldq, 0.f);
+  for (int f = 0; f < 9; ++f)
+    for (int ni = 0; ni < c->K; ++ni) {
+      const int e = c->new2old[ni];
+      std::memcpy(h.data() + f * c->ldq + size_t(ni) * c->Np, in + f * nodes + size_t(e) * c->Np, c->Np * sizeof(float));
+    }
+  CUDA_TRY(c, cudaMemcpyAsync(c->qbuf[c->cur] + size_t(b) * 9 * c->ldq, h.data(), h.size() * sizeof(float),
+                              cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return NEXD_OK;
+}
+
+int nexd_last_error(const nexd_ctx* c, char* buf, size_t len) {
+  if (!buf || len == 0) return NEXD_ERR_INVALID;
+  const std::string& m = c ? c->err : g_create_error;
+  std::strncpy(buf, m.c_str(), len - 1);
+  buf[len - 1] = '\0';
+  return NEXD_OK;
+}
+
+int nexd_launch_count(const nexd_ctx* c, int64_t* out) {
+  if (!c || !out) return NEXD_ERR_INVALID;
+  *out = c->launches;
+  return NEXD_OK;
+}
+
+int nexd_destroy(nexd_ctx* c) {
+  if (!c) return NEXD_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void* p : c->allocations) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return NEXD_OK;
+}
+
+}  // extern "C"

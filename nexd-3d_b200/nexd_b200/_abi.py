@@ -1,0 +1,115 @@
+"""ctypes mirror of include/nexd.h and include/nexd_host.h.
+
+The structures below are field-for-field copies of the C declarations; the
+shared libraries are the in-tree builds under ``nexd-3d_b200/lib``.
+"""
+import ctypes as C
+import os
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_DIR = os.path.join(PKG_ROOT, "lib")
+
+NEXD_OK = 0
+NEXD_ERR_INVALID = 1
+NEXD_ERR_CUDA = 2
+NEXD_ERR_NOMEM = 3
+NEXD_ERR_UNSUPPORTED = 4
+NEXD_ERR_NONFINITE = 5
+NEXD_ERR_NODEVICE = 6
+NEXD_NCOMP = 9
+NEXD_ABI_VERSION = 1
+
+_pd = C.POINTER(C.c_double)
+_pi = C.POINTER(C.c_int32)
+
+
+class NexdDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("N", C.c_int32), ("Np", C.c_int32), ("NpF", C.c_int32),
+        ("nelem", C.c_int32), ("nMB", C.c_int32), ("attenuation", C.c_int32), ("set_pml", C.c_int32),
+        ("timeint", C.c_int32), ("nt", C.c_int32), ("dt", C.c_double), ("init_value", C.c_double),
+        ("Dr", _pd), ("Ds", _pd), ("Dt", _pd), ("lift", _pd), ("invmass", _pd), ("fmask", _pi),
+        ("metric", _pd), ("jacobian", _pd), ("fscale", _pd), ("nnormal", _pd), ("stangential", _pd),
+        ("ttangential", _pd),
+        ("rho", _pd), ("vpu", _pd), ("vsu", _pd), ("lambdau", _pd), ("muu", _pd), ("ylambda", _pd),
+        ("ymu", _pd), ("wl", _pd),
+        ("neighbor", _pi), ("face", _pi), ("ibn", _pi),
+        ("pmlcheck", _pi), ("pml_profiles", _pd),
+        ("nsrc", C.c_int32), ("srcelem", _pi), ("srctype", _pi), ("srcInt", _pd), ("srcangle_force", _pd),
+        ("srcM", _pd), ("stf_per_step", C.c_int32), ("stf", _pd),
+        ("nrec", C.c_int32), ("recelem", _pi), ("recInt", _pd),
+        ("nbatch", C.c_int32), ("srcbatch", _pi),
+    ]
+
+
+class NexdBuildOpts(C.Structure):
+    _fields_ = [
+        ("N", C.c_int32), ("timeint", C.c_int32), ("cfl", C.c_double), ("nt", C.c_int32), ("t0", C.c_double),
+        ("stf_stage_time", C.c_int32), ("init_value", C.c_double), ("nbatch", C.c_int32),
+    ]
+
+
+class NexdMeshInfo(C.Structure):
+    _fields_ = [
+        ("dtfactor", C.c_double), ("dt", C.c_double), ("minGLL", C.c_double), ("cfl", C.c_double),
+        ("nglob", C.c_int32), ("ncoord", C.c_int32), ("vx", _pd), ("vy", _pd), ("vz", _pd), ("mass", _pd),
+        ("vdm", _pd), ("src_rst", _pd), ("rec_rst", _pd), ("recnr", _pi), ("mu", _pd), ("lambda_", _pd),
+        ("n_warnings", C.c_int32),
+    ]
+
+
+# Entry points declared in include/*.h, per library (checked by the CPU tests).
+HOST_SYMBOLS = ["nexd_mesh_build", "nexd_mesh_desc", "nexd_mesh_get_info", "nexd_mesh_write_seismograms",
+                "nexd_mesh_last_error", "nexd_mesh_free"]
+GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
+               "nexd_last_error", "nexd_launch_count", "nexd_destroy"]
+
+_host = None
+_gpu = None
+
+
+def _load(name):
+    path = os.path.join(LIB_DIR, name)
+    if not os.path.exists(path):
+        raise RuntimeError(f"{name} is not built ({path} missing); run __graft_entry__.build()")
+    return C.CDLL(path)
+
+
+def host_lib():
+    global _host
+    if _host is None:
+        lib = _load("libnexd_host.so")
+        lib.nexd_mesh_build.argtypes = [C.c_char_p, C.POINTER(NexdBuildOpts), C.POINTER(C.c_void_p)]
+        lib.nexd_mesh_build.restype = C.c_int
+        lib.nexd_mesh_desc.argtypes = [C.c_void_p]
+        lib.nexd_mesh_desc.restype = C.POINTER(NexdDesc)
+        lib.nexd_mesh_get_info.argtypes = [C.c_void_p, C.POINTER(NexdMeshInfo)]
+        lib.nexd_mesh_get_info.restype = C.c_int
+        lib.nexd_mesh_write_seismograms.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_float), C.c_int32,
+                                                    C.c_int32]
+        lib.nexd_mesh_write_seismograms.restype = C.c_int
+        lib.nexd_mesh_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        lib.nexd_mesh_last_error.restype = C.c_int
+        lib.nexd_mesh_free.argtypes = [C.c_void_p]
+        lib.nexd_mesh_free.restype = None
+        _host = lib
+    return _host
+
+
+def gpu_lib():
+    global _gpu
+    if _gpu is None:
+        lib = _load("libnexd.so")
+        vp = C.c_void_p
+        lib.nexd_create.argtypes = [C.POINTER(NexdDesc), C.POINTER(vp)]
+        lib.nexd_run.argtypes = [vp, C.c_int32, C.c_int32]
+        lib.nexd_get_traces.argtypes = [vp, C.POINTER(C.c_float)]
+        lib.nexd_get_field.argtypes = [vp, C.c_int32, C.POINTER(C.c_float)]
+        lib.nexd_set_field.argtypes = [vp, C.c_int32, C.POINTER(C.c_float)]
+        lib.nexd_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+        lib.nexd_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
+        lib.nexd_destroy.argtypes = [vp]
+        for n in GPU_SYMBOLS:
+            getattr(lib, n).restype = C.c_int
+        _gpu = lib
+    return _gpu

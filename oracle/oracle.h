@@ -1,0 +1,41 @@
+/*
+ * oracle.h -- CPU oracle for the NEXD-3D time loop (TEST INFRASTRUCTURE).
+ *
+ * A C++ restatement of subroutine timeloop3D (src/timeloopMod.f90:42-674)
+ * with waveMod (src/waveMod.f90:29-405) and rungekuttaMod
+ * (src/rungekuttaMod.f90:27-120), run on the same nexd_desc the GPU library
+ * consumes.  It is the checker for the GPU path: only the tests, the smoke
+ * check and the CPU-baseline leg of bench.py call it.  Nothing in the
+ * product (libnexd.so, libnexd_host.so, the nexd_b200 package) links or
+ * calls it.
+ *
+ * Pinning: in FP32 with the reference's RK2 it reproduces the reference's
+ * own golden seismograms simulations/brick/ref/seismo.* (see tests).
+ */
+#ifndef NEXD_ORACLE_H
+#define NEXD_ORACLE_H
+
+#include "../include/nexd.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Runs steps 1..it_end.  precision: 32 or 64.  traces: (nrec,nt,9,nbatch),
+ * zero-filled beyond it_end.  field (may be NULL): final q, (K*Np,9,nbatch)
+ * in FP64.  nthreads <= 0 uses all OpenMP threads.  Returns 0 or an error
+ * code (message via oracle_last_error). */
+int oracle_run(const nexd_desc* d, int precision, int it_end, float* traces, double* field, int nthreads);
+
+/* One right-hand side evaluation rq = L(q) for batch member 0 at step `it`
+ * (1-based) and stage `stage` (0-based), with q given as (K*Np,9) FP64 and
+ * the anelastic / PML auxiliaries set to `aux_value`.  rq out: (K*Np,9). */
+int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const double* q, double* rq);
+
+int oracle_last_error(char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,156 @@
+"""GPU (libnexd.so, sm_100a, FP32) against the CPU oracle (FP64) and against
+the reference's golden seismograms, through the C-ABI.
+
+Tolerances: receiver traces within 1e-4 relative L2 of the FP64 oracle
+(normalised per receiver and trace kind over its three components); a single
+right-hand side within 2e-5 relative to the field's RHS norm (FP32 rounding of
+O(Np) sums); golden brick traces within 2e-4 (the reference ran in FP32 with
+FP32 operators).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import (brick_dt_cfl, pin_brick_edge_stations, rel_l2, run_oracle, trace_misfit, write_brick)
+from nexd_b200 import Mesh, NexdError, synth
+from nexd_b200 import _abi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def Solver():
+    from nexd_b200.solver import Solver as S
+    return S
+
+
+def _rhs_case(tmp_path, kind, N):
+    d = str(tmp_path / f"{kind}{N}")
+    if kind == "elastic":
+        synth.write_cube(d, cells=3, nt=4)
+    else:
+        synth.write_twolayer(d, cells=(6, 6, 3), nt=4, nrec=4, attenuation=(kind != "pml"),
+                             pml=(kind != "anelastic"))
+    return Mesh(d, N=N, timeint=1)
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("kind", ["elastic", "anelastic", "pml", "anelastic_pml"])
+def test_single_rhs_matches_oracle(tmp_path, oracle, Solver, kind, N):
+    """One forward-Euler step from a random wavefield isolates one right-hand
+    side: (q1 - q0)/dt on the GPU equals the oracle's L(q0)."""
+    m = _rhs_case(tmp_path, kind, N)
+    rng = np.random.default_rng(N)
+    ng = m.K * m.Np
+    scale = np.array([1e6] * 6 + [1e-3] * 3)
+    q0 = (rng.standard_normal((ng, 9)) * scale).astype(np.float32)
+    q0 = np.asfortranarray(q0)
+    s = Solver(m.desc_ptr)
+    s.set_field(q0)
+    s.run(1, 1)
+    q1 = s.field().astype(np.float64)
+    rhs_gpu = (q1 - q0.astype(np.float64)) / np.float32(m.dt)
+    rq = np.zeros((ng, 9), order="F")
+    qd = np.asfortranarray(q0.astype(np.float64))
+    assert oracle.oracle_rhs(m.desc_ptr, 64, 1, 0, qd.ctypes.data_as(C.c_void_p), rq.ctypes.data_as(C.c_void_p)) == 0
+    for c0, c1 in ((0, 6), (6, 9)):
+        err = rel_l2(rhs_gpu[:, c0:c1], rq[:, c0:c1])
+        # the Euler difference loses digits: |q0| >> dt |L q0| for the stresses
+        tol = 2e-5 + 4 * np.finfo(np.float32).eps * np.linalg.norm(q0[:, c0:c1]) / (
+            m.dt * np.linalg.norm(rq[:, c0:c1]))
+        assert err < tol, (kind, N, c0, err, tol)
+
+
+def test_cube_lserk4_traces(tmp_path, oracle, Solver):
+    """Homogeneous 2 km cube, 6,000 tets, N=3, LSERK4: 400 steps (through the
+    first P and S arrivals at the surface receivers), FP32 GPU vs FP64 oracle."""
+    d = str(tmp_path / "cube")
+    synth.write_cube(d, nt=400)
+    m = Mesh(d, N=3, stf_stage_time=True)
+    s = Solver(m.desc_ptr)
+    s.run(1, 200)
+    s.run(201, 400)
+    tg = s.traces()[..., 0]
+    to = run_oracle(oracle, m, 64)[..., 0]
+    assert np.abs(to).max() > 1e-12  # the wave reached the receivers
+    assert trace_misfit(tg, to) < 1e-4
+
+
+def test_twolayer_anelastic_pml_traces(tmp_path, oracle, Solver):
+    """Two-layer Zener + NPML model (N=4, 10x10x5 cells = 3,000 tets), LSERK4,
+    moment-tensor source: 150 steps, FP32 GPU vs FP64 oracle."""
+    d = str(tmp_path / "tl")
+    synth.write_twolayer(d, cells=(10, 10, 5), nt=150, nrec=12, src_depth=(900.0, 900.0))
+    m = Mesh(d, N=4, stf_stage_time=True)
+    assert m.array("pmlcheck").sum() > 0 and m.desc.attenuation == 1
+    s = Solver(m.desc_ptr)
+    s.run(1, 150)
+    tg = s.traces()[..., 0]
+    tg_f = s.field()
+    to, fo = run_oracle(oracle, m, 64, want_field=True)
+    assert trace_misfit(tg, to[..., 0]) < 1e-4
+    assert rel_l2(tg_f, fo[..., 0]) < 1e-4
+
+
+@pytest.mark.parametrize("timeint", [1, 2, 3])
+def test_reference_integrators(tmp_path, oracle, Solver, timeint):
+    """The reference's Euler / TVD-RK2 / TVD-RK3 stage updates
+    (src/rungekuttaMod.f90:27-120) on the GPU vs the oracle."""
+    d = str(tmp_path / f"ti{timeint}")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=60, nrec=5, src_depth=(800.0, 800.0))
+    m = Mesh(d, N=3, timeint=timeint, cfl=0.1 if timeint == 1 else 0.3)
+    s = Solver(m.desc_ptr)
+    s.run(1, 60)
+    assert trace_misfit(s.traces()[..., 0], run_oracle(oracle, m, 64)[..., 0]) < 1e-4
+
+
+def test_brick_golden_on_gpu(tmp_path, Solver):
+    """The reference's own brick example (9,859 tets, N=4, RK2, 1000 steps) on
+    the GPU reproduces its golden seismograms within 2e-4 relative L2."""
+    golden, _ = write_brick(str(tmp_path))
+    m = Mesh(str(tmp_path), N=4, cfl=brick_dt_cfl())
+    pin_brick_edge_stations(m)
+    s = Solver(m.desc_ptr)
+    s.run(1, 1000)
+    tr = s.traces()[..., 0]
+    assert trace_misfit(tr, golden) < 2e-4
+
+
+def test_batched_wavefields(tmp_path, Solver):
+    """nbatch independent wavefields in one launch equal separate runs."""
+    d = str(tmp_path / "b")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=80, nrec=4, nsrc=3, src_depth=(700.0, 1200.0))
+    mb = Mesh(d, N=3, nbatch=3, stf_stage_time=True)
+    sb = Solver(mb.desc_ptr)
+    sb.run(1, 80)
+    tb = sb.traces()
+    for b in range(3):
+        ms = Mesh(d, N=3, nbatch=3, stf_stage_time=True)
+        # keep only source b: move the others to a wavefield that is not compared
+        srcb = ms.array("srcbatch")
+        stf = ms.array("stf")
+        for i in range(3):
+            if i != b:
+                stf[:, :, i] = 0.0
+        ss = Solver(ms.desc_ptr)
+        ss.run(1, 80)
+        ts = ss.traces()
+        assert rel_l2(tb[..., b], ts[..., b]) < 1e-6
+        assert srcb[b] == b
+
+
+def test_step_range_and_nonfinite_errors(tmp_path, Solver):
+    d = str(tmp_path / "e")
+    synth.write_cube(d, cells=2, nt=5)
+    m = Mesh(d, N=2)
+    s = Solver(m.desc_ptr)
+    with pytest.raises(NexdError) as ei:
+        s.run(1, 6)
+    assert ei.value.status == _abi.NEXD_ERR_INVALID
+    q = s.field()
+    q[:, 6] = np.nan
+    s.set_field(q)
+    with pytest.raises(NexdError) as ei:
+        s.run(1, 2)
+    assert ei.value.status == _abi.NEXD_ERR_NONFINITE

@@ -1,0 +1,99 @@
+"""The CPU oracle (oracle/liboracle.so) pinned against the reference's own
+golden seismograms and checked for the properties the method guarantees."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import (brick_dt_cfl, pin_brick_edge_stations, run_oracle, trace_misfit, write_brick, rel_l2)
+from nexd_b200 import Mesh, synth
+
+
+@pytest.fixture(scope="module")
+def brick_dir(tmp_path_factory, built):
+    d = tmp_path_factory.mktemp("brick")
+    golden, time = write_brick(str(d))
+    return str(d), golden, time
+
+
+def test_brick_golden_fp32_rk2(brick_dir, oracle):
+    """FP32 + the reference's TVD-RK2 reproduces simulations/brick/ref (33 traces
+    x 3 kinds, 1000 steps) at every station within 2e-4 relative L2.
+
+    Golden traces come from the reference run on 12 MPI ranks; the
+    partitioning moves halo copies only, not arithmetic.  Stations 1 and 11 sit
+    on mesh vertices shared by six elements; the reference's choice of element
+    is pinned (see conftest.BRICK_EDGE_STATIONS)."""
+    d, golden, time = brick_dir
+    m = Mesh(d, N=4, cfl=brick_dt_cfl())
+    assert abs(m.dt - 6.46257467e-06) < 1e-15
+    pin_brick_edge_stations(m)
+    tr = run_oracle(oracle, m, precision=32)[..., 0]
+    assert tr.shape == golden.shape
+    worst = trace_misfit(tr, golden)
+    assert worst < 2e-4, worst
+    # first sample: the start value 1e-24 interpolated (src/timeloopMod.f90:184-195)
+    assert np.allclose(tr[:, 0, :], golden[:, 0, :], rtol=1e-5, atol=0)
+
+
+def _cube(tmp_path, cells=2, N=2, nt=40, **kw):
+    d = str(tmp_path / f"cube_{cells}_{N}")
+    synth.write_cube(d, cells=cells, nt=nt)
+    return Mesh(d, N=N, **kw)
+
+
+def test_fp32_tracks_fp64(tmp_path, oracle):
+    m = _cube(tmp_path, cells=3, N=3, nt=200, stf_stage_time=True)
+    t64 = run_oracle(oracle, m, 64)
+    t32 = run_oracle(oracle, m, 32)
+    assert trace_misfit(t32[..., 0], t64[..., 0]) < 1e-4
+
+
+def test_constant_state_interior_rhs_vanishes(tmp_path, oracle):
+    """A constant wavefield has zero volume derivative and zero jumps, so the
+    right-hand side vanishes on elements with only interior faces."""
+    m = _cube(tmp_path, cells=3, N=3, nt=5)
+    ng = m.K * m.Np
+    q = np.zeros((ng, 9), order="F")
+    q[:] = np.array([1.0, -2.0, 0.5, 0.3, -0.7, 0.2, 1e-3, -2e-3, 5e-4])
+    rq = np.zeros_like(q)
+    st = oracle.oracle_rhs(m.desc_ptr, 64, 1, 0, q.ctypes.data_as(C.c_void_p), rq.ctypes.data_as(C.c_void_p))
+    assert st == 0
+    nb = m.array("neighbor")
+    src = set(m.array("srcelem") - 1)
+    interior = [e for e in range(m.K) if (nb[:, e] > 0).all() and e not in src]
+    assert interior
+    scale = np.abs(q).max() * 4000 / 100.0
+    for e in interior:
+        assert np.abs(rq[e * m.Np:(e + 1) * m.Np]).max() < 1e-9 * scale
+
+
+def test_lserk4_fourth_order_in_time(tmp_path, oracle):
+    """Halving dt divides the LSERK4 error by ~16 (Carpenter & Kennedy 1994):
+    traces at common times of runs with cfl c, c/2, c/4, with the source time
+    function sampled at the stage times."""
+    runs = []
+    for k, cfl in enumerate((0.2, 0.1, 0.05)):
+        d = str(tmp_path / f"conv{k}")
+        synth.write_cube(d, cells=2, nt=80 * 2 ** k)
+        m = Mesh(d, N=3, cfl=cfl, stf_stage_time=True, t0=0.1)
+        _, field = run_oracle(oracle, m, 64, want_field=True)
+        runs.append(field[..., 0])
+    e1 = np.linalg.norm(runs[0] - runs[2])
+    e2 = np.linalg.norm(runs[1] - runs[2])
+    ratio = e1 / e2
+    # e(c)/e(c/2) with the c/4 run as reference: (16-1)/(1-1/16)... ~ 17 for order 4
+    assert 10.0 < ratio < 25.0, ratio
+
+
+def test_batch_members_are_independent(tmp_path, oracle):
+    """Two wavefields sharing the mesh, one source each, equal two separate runs."""
+    d = str(tmp_path / "b2")
+    synth.write_twolayer(d, cells=(4, 4, 2), nt=30, nrec=3, nsrc=2, attenuation=False, pml=False,
+                         src_depth=(900.0, 1200.0))
+    mb = Mesh(d, N=2, nbatch=2)
+    tb = run_oracle(oracle, mb, 64)
+    ms = Mesh(d, N=2, nbatch=1)
+    ts = run_oracle(oracle, ms, 64)[..., 0]
+    # the single run has both sources in one wavefield: linear superposition
+    assert rel_l2(tb[..., 0] + tb[..., 1], ts) < 1e-5
