@@ -1,0 +1,282 @@
+"""Throughput of the NEXD-3D time-stepping hot path on B200.
+
+Workload: the two-layer anelastic model with NPML (4 x 4 x 2 km, 40x40x20
+hexahedra x 6 = 192,000 tets, N=4, 3 Zener mechanisms, 3-cell NPML on the
+sides and bottom, free top, seeded double-couple source, 100 surface
+receivers, LSERK4), synthetic and seeded.  A step is one LSERK4 time step
+(5 stages) over the whole mesh.  Metric: DOF-stage updates per second,
+9 * Np * K * stages * steps / time (only the 9 velocity-stress fields count).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: device time (CUDA events on the library's stream) of K steps with the
+state resident in HBM (the ~4 GB of wavefield, residual, memory-variable and
+NPML arrays exceed the 126 MB L2 on every step).  e2e: K steps through the
+C-ABI streaming call nexd_step_io, each step copying its source samples in
+from the host and its receiver samples out, wall clock.  Under torchrun each
+rank runs an independent replica (its own seeded source); the time is the
+maximum over ranks.  --impl reference times the CPU restatement of the
+reference's solver (the oracle, FP32 like the reference) on the host cores.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "nexd-3d_b200")
+sys.path.insert(0, PKG)
+
+from nexd_b200 import Mesh, synth, _abi  # noqa: E402
+
+WORKLOAD = "twolayer_anelastic_npml_192k_tets_N4_lserk4"
+CELLS = (40, 40, 20)
+N_ORDER = 4
+NT = 3000
+# CPU sample: same model family and order at 20x20x10 cells (24,000 tets)
+CPU_SAMPLE_CELLS = (20, 20, 10)
+CPU_SAMPLE_STEPS = 6
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from datetime import timedelta
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return rank, ws, local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(mesh, kind, elements):
+    """Compulsory DRAM bytes of one stage launch: every stored field-node is
+    read and written twice per LSERK stage (wavefield in/out, residual in/out:
+    16 B in FP32), plus per-element constants (~40 words) and, for NPML
+    elements, the 9 damping profiles per node (read once)."""
+    Np = mesh.Np
+    fields = 9 + (6 * mesh.desc.nMB if mesh.desc.attenuation else 0)
+    per = Np * fields * 16 + 160
+    if kind == "stage_pml":
+        per += Np * 27 * 16 + Np * 9 * 4
+    return per * elements
+
+
+def sample_clocks(stop_file, out_file):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        return subprocess.Popen(cmd, stdout=open(out_file, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None
+
+
+def summarize_clocks(path, device):
+    try:
+        rows = [l.split(",") for l in open(path).read().splitlines() if l.strip()]
+    except Exception:
+        return None
+    rows = [[x.strip() for x in r] for r in rows if len(r) >= 9 and r[0].strip() == str(device)]
+    if not rows:
+        return None
+    sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+    reasons = set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for r in rows:
+        for i, n in enumerate(names):
+            if r[5 + i].lower().startswith("active"):
+                reasons.add(n)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]) if rows else None,
+            "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def oracle_baseline(tmp, steps=CPU_SAMPLE_STEPS):
+    """FP32 CPU restatement of the reference solver on a bounded sample."""
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    lib.oracle_run.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_void_p, C.c_int]
+    d = os.path.join(tmp, "cpu_sample")
+    synth.write_twolayer(d, cells=CPU_SAMPLE_CELLS, nt=steps)
+    m = Mesh(d, N=N_ORDER, stf_stage_time=True)
+    tr = np.zeros((m.nrec, m.nt, 9, m.nbatch), dtype=np.float32, order="F")
+    t0 = time.perf_counter()
+    st = lib.oracle_run(m.desc_ptr, 32, steps, tr.ctypes.data_as(C.POINTER(C.c_float)), None, 0)
+    el = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError(f"oracle failed: {st}")
+    units = 9 * m.Np * m.K * 5 * steps
+    cores = os.cpu_count() or 1
+    sample = (f"{steps} LSERK4 steps of the same model family at {CPU_SAMPLE_CELLS[0]}x{CPU_SAMPLE_CELLS[1]}x"
+              f"{CPU_SAMPLE_CELLS[2]} cells ({m.K} tets, N={N_ORDER}, anelastic + NPML), FP32, "
+              f"{cores} OpenMP threads, {el:.1f} s")
+    return units / el, cores, sample
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", default="40,40,20", help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
+    args = ap.parse_args()
+    rank, world, local, dist = dist_init()
+    cells = tuple(int(x) for x in args.cells.split(","))
+    workload = WORKLOAD if cells == CELLS else f"twolayer_anelastic_npml_{6 * cells[0] * cells[1] * cells[2]}_tets_N4_lserk4"
+    steps, warmup = args.steps, max(3, args.warmup)
+    tmp = tempfile.mkdtemp(prefix=f"nexd_bench_{rank}_")
+    metric = "DOF-stage updates/s"
+    try:
+        if args.impl == "reference":
+            if rank == 0:
+                v, cores, sample = oracle_baseline(tmp)
+                line = {"metric": metric, "value": v, "unit": "DOF-stage/s", "n_gpus": args.gpus, "steps": steps,
+                        "warmup": warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                        "config": {"workload": workload, "sample": "see cpu_baseline"}, "impl": "reference",
+                        "cpu_baseline": {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port",
+                                         "sample": sample},
+                        "e2e": {"value": v, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                print(json.dumps(line), flush=True)
+            return
+        from nexd_b200.solver import Solver
+        import torch
+        if dist is None:
+            torch.cuda.set_device(0)
+        d = os.path.join(tmp, "model")
+        synth.write_twolayer(d, cells=cells, nt=NT, nrec=100, src_seed=2 + rank)
+        mesh = Mesh(d, N=N_ORDER, stf_stage_time=True)
+        s = Solver(mesh.desc_ptr)
+        nstage = 5
+        need = warmup + 2 * steps
+        if need > mesh.nt:
+            raise SystemExit(f"--warmup + 2*--steps must be <= {mesh.nt}")
+        s.run(1, warmup)
+        barrier(dist)
+        torch.cuda.synchronize()
+        clk_file = os.path.join(tmp, "clocks.csv")
+        clk = sample_clocks(None, clk_file) if rank == 0 else None
+        time.sleep(0.3 if clk else 0)
+        l0 = s.launch_count()
+        s.profile(True)
+        barrier(dist)
+        s.run(warmup + 1, warmup + steps)
+        torch.cuda.synchronize()
+        prof = s.profile()
+        launches = s.launch_count() - l0
+        s.profile(False)
+        if clk:
+            clk.terminate()
+            clk.wait()
+        dev_ms = max_over_ranks(dist, prof["span_ms"])
+        units = 9 * mesh.Np * mesh.K * nstage * steps
+        total_units = sum_over_ranks(dist, units)
+        value = total_units / (dev_ms * 1e-3)
+        # end to end through the streaming C-ABI call, host buffers in and out
+        nspt, nsrc, nrec = mesh.desc.stf_per_step, mesh.nsrc, mesh.nrec
+        stf_all = mesh.array("stf")  # (nspt, nt, nsrc)
+        stf_in = np.zeros((nspt, nsrc), dtype=np.float32, order="F")
+        tr_out = np.zeros((nrec, 9, mesh.nbatch), dtype=np.float32, order="F")
+        barrier(dist)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for it in range(warmup + steps + 1, warmup + 2 * steps + 1):
+            stf_in[:, :] = stf_all[:, it - 1, :]
+            s.step_io(it, stf_in, tr_out)
+        e2e_s = max_over_ranks(dist, time.perf_counter() - t0)
+        e2e = total_units / e2e_s
+        if rank != 0:
+            return
+        peak, peak_kind = load_peaks()
+        kinds = [k for k in ("stage_main", "stage_pml") if prof[k]["launches"] > 0]
+        dom = max(kinds, key=lambda k: prof[k]["ms"])
+        per_launch_ms = prof[dom]["ms"] / prof[dom]["launches"]
+        abytes = algorithmic_bytes(mesh, dom, prof[dom]["elements"])
+        achieved = abytes / (per_launch_ms * 1e-3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tp):
+            try:
+                t = json.load(open(tp)).get(workload, {}).get(dom)
+                traffic = None if t is None else float(t)
+            except Exception:
+                traffic = None
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            v, cores, sample = oracle_baseline(tmp)
+            cpu = {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
+        clocks = summarize_clocks(clk_file, local) if clk else None
+        state_gb = (2 * 9 + 9 + 2 * 6 * mesh.desc.nMB) * mesh.K * mesh.Np * 4 / 1e9
+        line = {
+            "metric": metric, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded two-layer model, per-rank seeded source)",
+            "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
+                       "integrator": "LSERK4 (5 stages)", "pml_tets": int(prof["stage_pml"]["elements"]),
+                       "receivers": nrec, "sources_per_rank": nsrc,
+                       "l2": f"inputs larger than L2: {state_gb:.1f} GB of state streamed per stage",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": per_launch_ms},
+            "kernels": {k: {"launches": prof[k]["launches"], "ms": round(prof[k]["ms"], 3)}
+                        for k in ("record", "stage_pml", "stage_main")},
+            "e2e": {"value": e2e, "unit": "DOF-stage/s", "h2d_bytes_per_step": int(nspt * nsrc * 4),
+                    "d2h_bytes_per_step": int(nrec * 9 * mesh.nbatch * 4)},
+            "gpu_launches": int(launches),
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+        s.close()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

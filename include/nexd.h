@@ -147,6 +147,44 @@ int nexd_get_field(nexd_ctx* ctx, int32_t b, float* out);
 /* Overwrites the wavefield of batch member `b` from `in`, shape (K*Np, 9). */
 int nexd_set_field(nexd_ctx* ctx, int32_t b, const float* in);
 
+/* State arrays for nexd_get_state / nexd_set_state. */
+enum nexd_state {
+  NEXD_STATE_Q = 0,     /* q (K*Np, 9), src/timeloopMod.f90:107 */
+  NEXD_STATE_THETA = 1, /* theta (K*Np, 6, nMB), src/timeloopMod.f90:116 */
+  NEXD_STATE_PML = 2    /* fprime, gprime, hprime as (K*Np, 27); zero outside PML elements */
+};
+
+/* Copies state array `which` (enum nexd_state) of batch member `b` to `out`. */
+int nexd_get_state(nexd_ctx* ctx, int32_t which, int32_t b, float* out);
+
+/* Overwrites state array `which` of batch member `b` from `in` (for PML
+ * auxiliaries only the PML elements' rows are read). */
+int nexd_set_state(nexd_ctx* ctx, int32_t which, int32_t b, const float* in);
+
+/* Advances one time step `it` with host-supplied source samples and returns
+ * that step's receiver samples: the streaming form of one iteration of the
+ * hot loop (src/timeloopMod.f90:357-589) for hosts that produce the source
+ * time function on the fly.  stf_in: (stf_per_step, nsrc) samples of step it
+ * (replacing the descriptor's values for that step), may be NULL to keep
+ * them; traces_out: (nrec, 9, nbatch) samples recorded at the start of step
+ * it.  Host buffers are staged through pinned memory owned by the context. */
+int nexd_step_io(nexd_ctx* ctx, int32_t it, const float* stf_in, float* traces_out);
+
+/* Kernel kinds reported by nexd_profile_get. */
+enum nexd_kernel_kind { NEXD_K_RECORD = 0, NEXD_K_STAGE_PML = 1, NEXD_K_STAGE_MAIN = 2, NEXD_K_COUNT = 3 };
+
+typedef struct nexd_profile {
+  int64_t launches[NEXD_K_COUNT]; /* launches per kernel kind since profiling was enabled */
+  double ms[NEXD_K_COUNT];        /* summed device time (CUDA events on the library's stream) */
+  int64_t elements[NEXD_K_COUNT]; /* elements processed per launch (stage kernels) */
+  double span_ms;                 /* summed device time of whole nexd_run calls (first to last launch) */
+} nexd_profile;
+
+/* Enables (on != 0) or disables per-launch CUDA-event timing in nexd_run and
+ * resets the counters. */
+int nexd_profile_enable(nexd_ctx* ctx, int32_t on);
+int nexd_profile_get(const nexd_ctx* ctx, nexd_profile* out);
+
 /* Last error message of ctx (or of the last failed nexd_create when ctx is
  * NULL), NUL-terminated and truncated to len bytes. */
 int nexd_last_error(const nexd_ctx* ctx, char* buf, size_t len);

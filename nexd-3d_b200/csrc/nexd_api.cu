@@ -40,6 +40,7 @@ struct nexd_ctx {
   std::string err;
   int N = 0, Np = 0, NpF = 0, K = 0, nMB = 0, nt = 0, nstage = 1, timeint = 4, nbatch = 1;
   int Kpml = 0;  // PML elements occupy internal indices [0, Kpml)
+  int npat = 4;  // face pattern rows (4 own masks + neighbour maps)
   bool att = false, pml = false;
   double dt = 0.0;
   long long ldq = 0, ldt = 0, lda = 0;
@@ -51,7 +52,7 @@ struct nexd_ctx {
   int grid_pml = 0, grid_main = 0;
   size_t smem_pml = 0, smem_main = 0;
   // device arrays
-  float *D = nullptr, *L = nullptr, *geo = nullptr, *ael = nullptr, *wl = nullptr, *prof = nullptr;
+  float *D = nullptr, *L = nullptr, *geo = nullptr, *ael = nullptr, *wl = nullptr, *prof_dev = nullptr;
   int4 *nbr = nullptr, *fcode = nullptr;
   unsigned char* patterns = nullptr;
   float* qbuf[3] = {nullptr, nullptr, nullptr};
@@ -65,6 +66,16 @@ struct nexd_ctx {
   int cur = 0;  // index of the buffer holding the current wavefield
   int64_t launches = 0;
   std::vector<void*> allocations;
+  // profiling: CUDA events around each launch on `stream`
+  bool profiling = false;
+  std::vector<cudaEvent_t> events;
+  std::vector<int> ev_kind;  // kind of event pair i (events 2i, 2i+1)
+  int ev_used = 0;
+  cudaEvent_t span[2] = {nullptr, nullptr};
+  nexd_profile prof{};
+  // pinned staging for nexd_step_io
+  float* pinned = nullptr;
+  size_t pinned_floats = 0;
 };
 
 namespace {
@@ -115,11 +126,7 @@ int fill(nexd_ctx* c, float* p, size_t n, float v) {
 
 template <int N>
 size_t smem_bytes(bool pml) {
-  using O = Order<N>;
-  size_t f = 3 * O::Np * O::Np + O::NF * O::Np + O::E * GEO_STRIDE + O::E * O::Np * O::QS + O::E * O::NF * 4 +
-             O::E * 4 * O::GS;
-  if (pml) f += O::E * O::Np * O::CS;
-  return f * sizeof(float);
+  return size_t(Order<N>::smem_floats(pml)) * sizeof(float);
 }
 
 using KernelFn = void (*)(const StageArgs);
@@ -162,8 +169,10 @@ int validate(const nexd_desc* d) {
   if (!(d->dt > 0.0) || !std::isfinite(d->dt)) return set_err(nullptr, NEXD_ERR_INVALID, "dt must be positive");
   if (d->timeint < 1 || d->timeint > 4) return set_err(nullptr, NEXD_ERR_INVALID, "timeint must be 1..4");
   if (d->nbatch < 1) return set_err(nullptr, NEXD_ERR_INVALID, "nbatch must be >= 1");
-  if (d->attenuation && (d->nMB < 1 || d->nMB > 8 || !d->wl || !d->ylambda || !d->ymu))
-    return set_err(nullptr, NEXD_ERR_INVALID, "attenuation needs 1..8 mechanisms with wl/ylambda/ymu");
+  if (d->attenuation && (!d->wl || !d->ylambda || !d->ymu))
+    return set_err(nullptr, NEXD_ERR_INVALID, "attenuation needs wl/ylambda/ymu");
+  if (d->attenuation && d->nMB != nexd_dev::kNMB)
+    return set_err(nullptr, NEXD_ERR_UNSUPPORTED, "attenuation supports nMB = 3 Zener mechanisms (the reference's nMB)");
   if (d->set_pml && (!d->pmlcheck || !d->pml_profiles))
     return set_err(nullptr, NEXD_ERR_INVALID, "set_pml needs pmlcheck and pml_profiles");
   const void* req[] = {d->Dr, d->Ds, d->Dt, d->lift, d->fmask, d->metric, d->jacobian, d->fscale, d->nnormal,
@@ -282,7 +291,8 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
       h_fcode[4 * ni + f] = id;
     }
   }
-  if (patid.size() > 250) return fail(set_err(c, NEXD_ERR_UNSUPPORTED, "too many distinct face permutations"));
+  if (patid.size() + 4 > 64) return fail(set_err(c, NEXD_ERR_UNSUPPORTED, "too many distinct face permutations"));
+  c->npat = 4 + int(patid.size());
 
   // ---- element records ----
   std::vector<float> h_geo(size_t(K) * GEO_STRIDE, 0.f);
@@ -315,15 +325,25 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     g[G_AP] = float(1.0 / (lam + 2 * mu));
     g[G_AS] = float(1.0 / (2 * mu));
   }
-  std::vector<float> h_D(size_t(3) * Np * Np), h_L(size_t(NF) * Np);
+  std::vector<float> h_D(size_t(3) * Np * Np), h_L;
   for (int k = 0; k < Np; ++k)
     for (int n = 0; n < Np; ++n) {
       h_D[size_t(k) * Np + n] = float(d->Dr[size_t(k) * Np + n]);
       h_D[size_t(Np) * Np + size_t(k) * Np + n] = float(d->Ds[size_t(k) * Np + n]);
       h_D[size_t(2) * Np * Np + size_t(k) * Np + n] = float(d->Dt[size_t(k) * Np + n]);
     }
-  for (int j = 0; j < NF; ++j)
-    for (int n = 0; n < Np; ++n) h_L[size_t(j) * Np + n] = float(d->lift[size_t(j) * Np + n]);
+  {
+    // LIFT in face-node pairs: [face][pair][n][2], zero where NpF is odd
+    const int npair = (NpF + 1) / 2;
+    h_L.assign(size_t(4) * npair * Np * 2, 0.f);
+    for (int f = 0; f < 4; ++f)
+      for (int ip = 0; ip < npair; ++ip)
+        for (int n = 0; n < Np; ++n)
+          for (int h = 0; h < 2; ++h) {
+            const int i = 2 * ip + h;
+            if (i < NpF) h_L[((size_t(f) * npair + ip) * Np + n) * 2 + h] = float(d->lift[size_t(f * NpF + i) * Np + n]);
+          }
+  }
   std::vector<float> h_ael, h_wl;
   if (c->att) {
     h_ael.assign(size_t(K) * 3 * c->nMB, 0.f);
@@ -428,7 +448,7 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     if ((st = dalloc(c, &c->aux, n)) || (st = dalloc(c, &c->aux2, n))) return fail(st);
     CUDA_TRY(c, cudaMemset(c->aux, 0, n * sizeof(float)));
     CUDA_TRY(c, cudaMemset(c->aux2, 0, n * sizeof(float)));
-    if ((st = upload(c, &c->prof, h_prof))) return fail(st);
+    if ((st = upload(c, &c->prof_dev, h_prof))) return fail(st);
   }
   if ((st = upload(c, &c->src_head, h_head)) || (st = upload(c, &c->src_next, h_next)) ||
       (st = upload(c, &c->src_batch, h_sb)) || (st = upload(c, &c->src_pat, h_spat)) || (st = upload(c, &c->stf, h_stf)))
@@ -477,9 +497,40 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   return NEXD_OK;
 }
 
-int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
-  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
-  if (it_begin < 1 || it_end > c->nt || it_begin > it_end) return set_err(c, NEXD_ERR_INVALID, "step range out of 1..nt");
+namespace {
+
+int ev_begin(nexd_ctx* c, int kind) {
+  if (!c->profiling) return -1;
+  const int pair = c->ev_used++;
+  while (int(c->events.size()) < 2 * c->ev_used) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    c->events.push_back(e);
+  }
+  if (int(c->ev_kind.size()) < c->ev_used) c->ev_kind.resize(c->ev_used);
+  c->ev_kind[pair] = kind;
+  cudaEventRecord(c->events[2 * pair], c->stream);
+  return pair;
+}
+
+void ev_end(nexd_ctx* c, int pair) {
+  if (pair >= 0) cudaEventRecord(c->events[2 * pair + 1], c->stream);
+}
+
+// Collects the timed pairs after the stream is synchronised.
+void ev_collect(nexd_ctx* c) {
+  for (int p = 0; p < c->ev_used; ++p) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->events[2 * p], c->events[2 * p + 1]) == cudaSuccess) {
+      c->prof.ms[c->ev_kind[p]] += ms;
+      c->prof.launches[c->ev_kind[p]] += 1;
+    }
+  }
+  c->ev_used = 0;
+}
+
+// Enqueues steps it_begin..it_end on the context's stream.
+void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
   const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
   size_t smem_p = 0, smem_m = 0;
   KernelFn kp = pick_kernel(c->N, c->att, true, mode, smem_p);
@@ -496,9 +547,10 @@ int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
   a.nbr = c->nbr;
   a.fcode = c->fcode;
   a.patterns = c->patterns;
+  a.npat = c->npat;
   a.ael = c->ael;
   a.wl = c->wl;
-  a.prof = c->prof;
+  a.prof = c->prof_dev;
   a.res = c->res;
   a.th = c->th;
   a.th2 = c->th2;
@@ -537,7 +589,9 @@ int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
       r.q = c->qbuf[c->cur];
       const int threads = 128;
       const int blocks = (rec_warps * 32 + threads - 1) / threads;
+      const int ev = ev_begin(c, NEXD_K_RECORD);
       record_kernel<<<blocks, threads, 0, c->stream>>>(r);
+      ev_end(c, ev);
       ++c->launches;
     }
     a.it = it;
@@ -571,24 +625,100 @@ int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
       if (c->Kpml > 0) {
         a.e_begin = 0;
         a.e_end = c->Kpml;
+        const int ev = ev_begin(c, NEXD_K_STAGE_PML);
         kp<<<c->grid_pml, 256, c->smem_pml, c->stream>>>(a);
+        ev_end(c, ev);
         ++c->launches;
       }
       if (c->K > c->Kpml) {
         a.e_begin = c->Kpml;
         a.e_end = c->K;
+        const int ev = ev_begin(c, NEXD_K_STAGE_MAIN);
         km<<<c->grid_main, 256, c->smem_main, c->stream>>>(a);
+        ev_end(c, ev);
         ++c->launches;
       }
       if (c->timeint == 4 || c->timeint == 1) c->cur = outb;
     }
   }
+}
+
+// Synchronises, collects profiling events and checks the non-finite flag.
+int finish(nexd_ctx* c) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   int flag = 0;
   CUDA_TRY(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (c->profiling) ev_collect(c);
   if (flag) return set_err(c, NEXD_ERR_NONFINITE, "non-finite value in the wavefield at a receiver");
+  return NEXD_OK;
+}
+
+}  // namespace
+
+int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (it_begin < 1 || it_end > c->nt || it_begin > it_end) return set_err(c, NEXD_ERR_INVALID, "step range out of 1..nt");
+  if (c->profiling) {
+    if (!c->span[0]) {
+      CUDA_TRY(c, cudaEventCreate(&c->span[0]));
+      CUDA_TRY(c, cudaEventCreate(&c->span[1]));
+    }
+    CUDA_TRY(c, cudaEventRecord(c->span[0], c->stream));
+  }
+  enqueue_steps(c, it_begin, it_end);
+  if (c->profiling) CUDA_TRY(c, cudaEventRecord(c->span[1], c->stream));
+  int st = finish(c);
+  if (c->profiling && st == NEXD_OK) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->span[0], c->span[1]) == cudaSuccess) c->prof.span_ms += ms;
+  }
+  return st;
+}
+
+int nexd_step_io(nexd_ctx* c, int32_t it, const float* stf_in, float* traces_out) {
+  if (!c || !traces_out) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  if (it < 1 || it > c->nt) return set_err(c, NEXD_ERR_INVALID, "step out of 1..nt");
+  const size_t nin = size_t(c->nspt) * c->nsrc, nout = size_t(c->nrec) * 9 * c->nbatch;
+  if (!c->pinned) {
+    c->pinned_floats = std::max<size_t>(1, nin + nout);
+    CUDA_TRY(c, cudaMallocHost(&c->pinned, c->pinned_floats * sizeof(float)));
+  }
+  if (stf_in && nin > 0) {
+    std::memcpy(c->pinned, stf_in, nin * sizeof(float));
+    // row s of (nspt, nsrc) goes to stf[s][it-1][:]
+    CUDA_TRY(c, cudaMemcpy2DAsync(c->stf + size_t(it - 1) * c->nspt, size_t(c->nt) * c->nspt * sizeof(float), c->pinned,
+                                  size_t(c->nspt) * sizeof(float), size_t(c->nspt) * sizeof(float), c->nsrc,
+                                  cudaMemcpyHostToDevice, c->stream));
+  }
+  enqueue_steps(c, it, it);
+  if (nout > 0) {
+    // (nrec, nt, 9*nbatch) column it-1 -> (nrec, 9*nbatch)
+    CUDA_TRY(c, cudaMemcpy2DAsync(c->pinned + nin, size_t(c->nrec) * sizeof(float),
+                                  c->traces + size_t(it - 1) * c->nrec, size_t(c->nt) * c->nrec * sizeof(float),
+                                  size_t(c->nrec) * sizeof(float), size_t(9) * c->nbatch, cudaMemcpyDeviceToHost,
+                                  c->stream));
+  }
+  int st = finish(c);
+  if (st) return st;
+  if (nout > 0) std::memcpy(traces_out, c->pinned + nin, nout * sizeof(float));
+  return NEXD_OK;
+}
+
+int nexd_profile_enable(nexd_ctx* c, int32_t on) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  c->profiling = on != 0;
+  c->prof = nexd_profile{};
+  c->prof.elements[NEXD_K_STAGE_PML] = c->Kpml;
+  c->prof.elements[NEXD_K_STAGE_MAIN] = c->K - c->Kpml;
+  c->ev_used = 0;
+  return NEXD_OK;
+}
+
+int nexd_profile_get(const nexd_ctx* c, nexd_profile* out) {
+  if (!c || !out) return NEXD_ERR_INVALID;
+  *out = c->prof;
   return NEXD_OK;
 }
 
@@ -601,37 +731,74 @@ int nexd_get_traces(nexd_ctx* c, float* out) {
   return NEXD_OK;
 }
 
-int nexd_get_field(nexd_ctx* c, int32_t b, float* out) {
-  if (!c || !out) return set_err(c, NEXD_ERR_INVALID, "null argument");
+namespace {
+// Device layout of a state array: (pointer to batch member b, fields, field stride, elements covered).
+int state_view(nexd_ctx* c, int32_t which, int32_t b, float** base, int* nf, long long* ld, int* nel) {
   if (b < 0 || b >= c->nbatch) return set_err(c, NEXD_ERR_INVALID, "batch index out of range");
+  if (which == NEXD_STATE_Q) {
+    *base = c->qbuf[c->cur] + size_t(b) * 9 * c->ldq;
+    *nf = 9; *ld = c->ldq; *nel = c->K;
+  } else if (which == NEXD_STATE_THETA) {
+    if (!c->att) return set_err(c, NEXD_ERR_INVALID, "no memory variables: attenuation is off");
+    *base = c->th + size_t(b) * 6 * c->nMB * c->ldt;
+    *nf = 6 * c->nMB; *ld = c->ldt; *nel = c->K;
+  } else if (which == NEXD_STATE_PML) {
+    if (!c->pml) return set_err(c, NEXD_ERR_INVALID, "no PML auxiliaries: set_pml is off");
+    *base = c->aux ? c->aux + size_t(b) * 27 * c->lda : nullptr;
+    *nf = 27; *ld = c->lda; *nel = c->Kpml;
+  } else {
+    return set_err(c, NEXD_ERR_INVALID, "unknown state array");
+  }
+  return NEXD_OK;
+}
+}  // namespace
+
+int nexd_get_state(nexd_ctx* c, int32_t which, int32_t b, float* out) {
+  if (!c || !out) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  float* base;
+  int nf, nel;
+  long long ld;
+  if (int st = state_view(c, which, b, &base, &nf, &ld, &nel)) return st;
   const size_t nodes = size_t(c->K) * c->Np;
-  std::vector<float> h(size_t(9) * c->ldq);
-  CUDA_TRY(c, cudaMemcpyAsync(h.data(), c->qbuf[c->cur] + size_t(b) * 9 * c->ldq, h.size() * sizeof(float),
-                              cudaMemcpyDeviceToHost, c->stream));
+  std::fill(out, out + nodes * nf, 0.f);
+  if (!base || nel == 0) return NEXD_OK;
+  std::vector<float> h(size_t(nf) * ld);
+  CUDA_TRY(c, cudaMemcpyAsync(h.data(), base, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  for (int f = 0; f < 9; ++f)
-    for (int ni = 0; ni < c->K; ++ni) {
+  for (int f = 0; f < nf; ++f)
+    for (int ni = 0; ni < nel; ++ni) {
       const int e = c->new2old[ni];
-      std::memcpy(out + f * nodes + size_t(e) * c->Np, h.data() + f * c->ldq + size_t(ni) * c->Np, c->Np * sizeof(float));
+      std::memcpy(out + f * nodes + size_t(e) * c->Np, h.data() + f * ld + size_t(ni) * c->Np, c->Np * sizeof(float));
     }
   return NEXD_OK;
 }
 
-int nexd_set_field(nexd_ctx* c, int32_t b, const float* in) {
+int nexd_set_state(nexd_ctx* c, int32_t which, int32_t b, const float* in) {
   if (!c || !in) return set_err(c, NEXD_ERR_INVALID, "null argument");
-  if (b < 0 || b >= c->nbatch) return set_err(c, NEXD_ERR_INVALID, "batch index out of range");
+  float* base;
+  int nf, nel;
+  long long ld;
+  if (int st = state_view(c, which, b, &base, &nf, &ld, &nel)) return st;
+  if (!base || nel == 0) return NEXD_OK;
   const size_t nodes = size_t(c->K) * c->Np;
-  std::vector<float> h(size_t(9) * c->ldq, 0.f);
-  for (int f = 0; f < 9; ++f)
-    for (int ni = 0; ni < c->K; ++ni) {
+  std::vector<float> h(size_t(nf) * ld, 0.f);
+  if (which != NEXD_STATE_Q) {  // keep padding / untouched rows as they are
+    CUDA_TRY(c, cudaMemcpyAsync(h.data(), base, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  for (int f = 0; f < nf; ++f)
+    for (int ni = 0; ni < nel; ++ni) {
       const int e = c->new2old[ni];
-      std::memcpy(h.data() + f * c->ldq + size_t(ni) * c->Np, in + f * nodes + size_t(e) * c->Np, c->Np * sizeof(float));
+      std::memcpy(h.data() + f * ld + size_t(ni) * c->Np, in + f * nodes + size_t(e) * c->Np, c->Np * sizeof(float));
     }
-  CUDA_TRY(c, cudaMemcpyAsync(c->qbuf[c->cur] + size_t(b) * 9 * c->ldq, h.data(), h.size() * sizeof(float),
-                              cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(base, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return NEXD_OK;
 }
+
+int nexd_get_field(nexd_ctx* c, int32_t b, float* out) { return nexd_get_state(c, NEXD_STATE_Q, b, out); }
+
+int nexd_set_field(nexd_ctx* c, int32_t b, const float* in) { return nexd_set_state(c, NEXD_STATE_Q, b, in); }
 
 int nexd_last_error(const nexd_ctx* c, char* buf, size_t len) {
   if (!buf || len == 0) return NEXD_ERR_INVALID;
@@ -651,6 +818,10 @@ int nexd_destroy(nexd_ctx* c) {
   if (!c) return NEXD_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (void* p : c->allocations) cudaFree(p);
+  for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->span)
+    if (e) cudaEventDestroy(e);
+  if (c->pinned) cudaFreeHost(c->pinned);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NEXD_OK;

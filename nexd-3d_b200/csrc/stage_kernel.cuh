@@ -42,7 +42,34 @@ struct Order {
   static constexpr int E = THREADS / Np;  // elements per chunk
   static constexpr int QS = 12;           // padded field stride of staged q (3 x float4)
   static constexpr int GS = 36;           // per-face expansion coefficients
-  static constexpr int CS = 28;           // padded contravariant-flux stride (PML)
+  static constexpr int CS = 34;           // contravariant-flux row stride (PML): r 0..9, s 10..19, t 20..29
+  // shared-memory section sizes in floats, each a multiple of 4 (float4 alignment)
+  static constexpr int r4(int x) { return (x + 3) / 4 * 4; }
+  static constexpr int SD = r4(3 * Np * Np);  // Dr, Ds, Dt as [d][k][n]
+  static constexpr int NPAIR = (NpF + 1) / 2;  // face-node pairs per face (last one zero-padded when NpF is odd)
+  static constexpr int NFP = 4 * 2 * NPAIR;     // padded face nodes per element
+  static constexpr int SL = 4 * NPAIR * Np * 2; // LIFT as [face][pair][n][2]
+  // one prefetch buffer: element records, own wavefield (field-major), the
+  // neighbour face traces and the connectivity of the following chunk
+  static constexpr int SGEO = E * 64;
+  static constexpr int SQF = r4(9 * E * Np);
+  static constexpr int STR = r4(E * NF * 9);
+  static constexpr int SIDS = r4(E * 12);
+  static constexpr int BUF = SGEO + SQF + STR + SIDS;
+  // per-element strides of the work areas are = 16 (mod 32) words, so the two
+  // elements that share a warp read different shared-memory banks
+  static constexpr int b16(int x) { return x + ((16 - x % 32) + 32) % 32; }
+  static constexpr int QE = b16(Np * QS);   // interleaved own wavefield per element
+  static constexpr int CFE = b16(Np * CS);  // contravariant fluxes per element (PML)
+  static constexpr int AE = b16(3 * NFP);   // amplitudes per element
+  static constexpr int SQI = E * QE;        // interleaved copy for the volume loop (non-PML)
+  static constexpr int SAMP = E * AE;       // amplitudes [e][comp][padded face node]
+  static constexpr int SG = E * 4 * GS;
+  static constexpr int SCF = E * CFE;
+  static constexpr int SPAT = r4(64 * NpF / 4 + 1);  // face patterns (bytes/4), up to 64 rows
+  static constexpr int smem_floats(bool pml) {
+    return SD + SL + 2 * BUF + (pml ? SCF : SQI) + SAMP + SG + SPAT;
+  }
 };
 
 // Per-element record, 64 floats.
@@ -75,11 +102,12 @@ struct StageArgs {
   long long ldt;       // field stride of theta arrays
   long long lda;       // field stride of PML auxiliary arrays (PML nodes)
   const float* D;      // [3][Np][Np] as D[d][k][n]
-  const float* L;      // [NF][Np] as L[j][n]
+  const float* L;      // [4][NPAIR][Np][2]: LIFT(n, face node) in face-node pairs
   const float* geo;    // [K][64]
   const int4* nbr;     // [K] internal neighbour per face, -1 on boundaries
   const int4* fcode;   // [K] per face: pattern id >= 0, -1 free, -2 absorbing
   const unsigned char* patterns;  // [npat][NpF] neighbour-local node of face node i
+  int npat;
   const float* ael;    // [K][3*nMB]: -lam*Ylam, -2mu*Ymu, sum (src/timeloopMod.f90:274-282)
   const float* wl;     // [nMB]
   const float* prof;   // [Kpml][9][Np]: ddx ddy ddz ax ay az kx ky kz
@@ -178,172 +206,330 @@ __device__ __forceinline__ void face_amplitudes(const float* g, int f, const flo
   }
 }
 
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Work item w of a launch: batch member and first element of the chunk.
+struct Chunk {
+  int b, e0, ne;
+};
+template <int E>
+__device__ __forceinline__ Chunk chunk_of(const StageArgs& a, int w, int nchunk) {
+  Chunk c;
+  c.b = w / nchunk;
+  c.e0 = a.e_begin + (w - c.b * nchunk) * E;
+  c.ne = min(E, a.e_end - c.e0);
+  return c;
+}
+
+// Issues the asynchronous copies of one chunk into a prefetch buffer:
+// element records (16-byte copies), own wavefield (field-major), the
+// neighbour face traces of interior faces (gathered through the face
+// patterns, using the connectivity `ids` staged one chunk earlier) and the
+// connectivity of the chunk after it (`next`, -1 for none).
+template <int N>
+__device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
+                                            const Chunk* next, const unsigned char* pat) {
+  using O = Order<N>;
+  constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  float* bGeo = buf;
+  float* bQ = bGeo + O::SGEO;
+  float* bTr = bQ + O::SQF;
+  int* bIds = reinterpret_cast<int*>(bTr + O::STR);
+  const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
+  for (int i = tid; i < c.ne * 16; i += nth) cp_async16(bGeo + 4 * i, a.geo + (long long)c.e0 * GEO_STRIDE + 4 * i);
+  const int cnt = c.ne * Np;
+  const long long base = (long long)c.e0 * Np;
+  for (int i = tid; i < 9 * E * Np; i += nth) {
+    const int f = i / (E * Np), r = i - f * (E * Np);
+    if (r < cnt) cp_async4(bQ + i, qin + f * a.ldq + base + r);
+  }
+  for (int i = tid; i < c.ne * NF; i += nth) {
+    const int ee = i / NF, j = i - ee * NF;
+    const int f = j / NpF, fi = j - f * NpF;
+    const int code = ids[ee * 12 + 4 + f];
+    if (code >= 0) {
+      const int nb = ids[ee * 12 + f];
+      const long long gn = (long long)nb * Np + pat[code * NpF + fi];
+      float* dst = bTr + i * 9;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) cp_async4(dst + k, qin + k * a.ldq + gn);
+    }
+  }
+  if (next)
+    for (int i = tid; i < next->ne * 2; i += nth) {
+      const int ee = i >> 1;
+      const int4* src = (i & 1) ? a.fcode + next->e0 + ee : a.nbr + next->e0 + ee;
+      cp_async16(bIds + ee * 12 + (i & 1) * 4, src);
+    }
+  // this chunk's own face codes (the face phase reads them from here)
+  for (int i = tid; i < c.ne; i += nth) cp_async16(bIds + i * 12 + 8, a.fcode + c.e0 + i);
+  cp_async_commit();
+}
+
+// Memory variables per mechanism set: the reference's nMB = 3 (src/constants.h:36).
+constexpr int kNMB = 3;
+
 template <int N, bool ATT, bool PML, int MODE>
-__global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
+__global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs a) {
   using O = Order<N>;
   constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, QS = O::QS, GS = O::GS, CS = O::CS;
   extern __shared__ __align__(16) float smem[];
-  float* sD = smem;                          // 3*Np*Np
-  float* sL = sD + 3 * Np * Np;              // NF*Np
-  float* sGeo = sL + NF * Np;                // E*64
-  float* sQ = sGeo + E * GEO_STRIDE;         // E*Np*QS
-  float* sAmp = sQ + E * Np * QS;            // E*NF*4
-  float* sG = sAmp + E * NF * 4;             // E*4*GS
-  float* sCF = sG + E * 4 * GS;              // PML: E*Np*CS
-  (void)sCF;
+  float* sD = smem;              // 3*Np*Np: D[d][k][n]
+  float* sL = sD + O::SD;        // LIFT in face-node pairs
+  float* sBuf = sL + O::SL;      // 2 prefetch buffers
+  float* sQI = sBuf + 2 * O::BUF;  // non-PML: interleaved own wavefield [e][k][QS]
+  float* sCF = sQI;              // PML: contravariant modified fluxes [e][k][CS]
+  float* sAmp = sQI + (PML ? O::SCF : O::SQI);  // E*3*NFP
+  float* sG = sAmp + O::SAMP;    // E*4*GS
+  unsigned char* sPat = reinterpret_cast<unsigned char*>(sG + O::SG);  // face patterns
 
   const int tid = threadIdx.x;
   for (int i = tid; i < 3 * Np * Np; i += blockDim.x) sD[i] = a.D[i];
-  for (int i = tid; i < NF * Np; i += blockDim.x) sL[i] = a.L[i];
+  for (int i = tid; i < O::SL; i += blockDim.x) sL[i] = a.L[i];
+  if (NpF & 1)  // padding slots of the amplitude pairs stay zero
+    for (int i = tid; i < E * 3 * 4; i += blockDim.x)
+      sAmp[(i >> 2) / 3 * O::AE + (i >> 2) % 3 * O::NFP + (i & 3) * 2 * O::NPAIR + NpF] = 0.f;
+  for (int i = tid; i < a.npat * NpF; i += blockDim.x) sPat[i] = a.patterns[i];
 
   const int nel = a.e_end - a.e_begin;
   const int nchunk = (nel + E - 1) / E;
   const int nwork = nchunk * a.nbatch;
   const int le = tid / Np;       // element of this thread within the chunk
   const int n = tid - le * Np;   // node of this thread
+  int w = blockIdx.x;
+  if (w >= nwork) return;
 
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const int b = w / nchunk;
-    const int e0 = a.e_begin + (w - b * nchunk) * E;
-    const int ne = min(E, a.e_end - e0);
-    const float* qin = a.q_in + (long long)b * 9 * a.ldq;
-    __syncthreads();  // previous chunk done with shared memory (and operators staged)
-    // ---- stage element records and own wavefield --------------------------------
-    for (int i = tid; i < ne * GEO_STRIDE; i += blockDim.x) sGeo[i] = a.geo[(long long)e0 * GEO_STRIDE + i];
-    {
-      const long long base = (long long)e0 * Np;
-      const int cnt = ne * Np;
-      for (int i = tid; i < 9 * cnt; i += blockDim.x) {
-        const int f = i / cnt, r = i - f * cnt;
-        sQ[r * QS + f] = qin[f * a.ldq + base + r];
-      }
+  // prologue: connectivity of the first chunk straight from global memory
+  {
+    const Chunk c0 = chunk_of<E>(a, w, nchunk);
+    const int wn = w + gridDim.x;
+    Chunk c1;
+    if (wn < nwork) c1 = chunk_of<E>(a, wn, nchunk);
+    int* ids0 = reinterpret_cast<int*>(sBuf + O::BUF + O::SGEO + O::SQF + O::STR);  // scratch: buffer 1's ids slot
+    for (int i = tid; i < c0.ne * 8; i += blockDim.x) {
+      const int ee = i >> 3, k = i & 7;
+      ids0[ee * 12 + k] = k < 4 ? reinterpret_cast<const int*>(a.nbr)[4 * (c0.e0 + ee) + k]
+                                : reinterpret_cast<const int*>(a.fcode)[4 * (c0.e0 + ee) + k - 4];
     }
     __syncthreads();
+    issue_chunk<N>(a, c0, ids0, sBuf, wn < nwork ? &c1 : nullptr, sPat);
+  }
+
+  for (int p = 0; w < nwork; w += gridDim.x, p ^= 1) {
+    const Chunk ch = chunk_of<E>(a, w, nchunk);
+    const int b = ch.b, e0 = ch.e0, ne = ch.ne;
+    float* buf = sBuf + p * O::BUF;
+    const float* sGeo = buf;
+    const float* sQF = buf + O::SGEO;
+    const float* sTr = sQF + O::SQF;
+    const int* sIds = reinterpret_cast<const int*>(sTr + O::STR);  // connectivity of the next chunk
+    cp_async_wait_all();
+    __syncthreads();  // this chunk's data is in `buf`; the other buffer and work areas are free
+
+    // ---- register prefetch of this node's update-phase state --------------------
+    // (all loads of the chunk are in flight while the face, volume and lift
+    // terms are computed; one block per SM keeps them in registers)
+    const bool active = le < ne;
+    const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
+    constexpr int NTH = ATT ? 6 * kNMB : 1;
+    constexpr int NAX = PML ? 27 : 1;
+    float pre_res[9], pre_th[NTH], pre_th2[NTH], pre_ax[NAX], pre_ax2[NAX], pre_pr[PML ? 9 : 1];
+    const bool need2 = (MODE == MODE_LSERK) || !a.stage_first;
+    if (active) {
+      if (MODE == MODE_LSERK) {
+        const float* rs = a.res + (long long)b * 9 * a.ldq + node;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) pre_res[c] = __ldcs(rs + c * a.ldq);
+      } else if (a.ca != 0.f) {
+        const float* qn = a.q_n + (long long)b * 9 * a.ldq + node;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) pre_res[c] = __ldcs(qn + c * a.ldq);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) pre_res[c] = 0.f;
+      }
+      if (ATT) {
+        const float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
+        const float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
+#pragma unroll
+        for (int j = 0; j < NTH; ++j) pre_th[j] = __ldcs(th + j * a.ldt);
+#pragma unroll
+        for (int j = 0; j < NTH; ++j) pre_th2[j] = need2 ? __ldcs(th2 + j * a.ldt) : 0.f;
+      }
+      if (PML) {
+        const long long pn = (long long)(e0 + le) * Np + n;  // PML elements come first internally
+        const float* ax = a.aux + (long long)b * 27 * a.lda + pn;
+        const float* ax2 = a.aux2 + (long long)b * 27 * a.lda + pn;
+        const float* pr = a.prof + (long long)(e0 + le) * 9 * Np + n;
+#pragma unroll
+        for (int i = 0; i < 27; ++i) pre_ax[i] = __ldcs(ax + i * a.lda);
+#pragma unroll
+        for (int i = 0; i < 27; ++i) pre_ax2[i] = need2 ? __ldcs(ax2 + i * a.lda) : 0.f;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) pre_pr[i] = __ldg(pr + i * Np);
+      }
+    }
+    // ---- start the next chunk's copies ------------------------------------------
+    {
+      const int wn = w + gridDim.x;
+      if (wn < nwork) {
+        const Chunk cn = chunk_of<E>(a, wn, nchunk);
+        const int wnn = wn + gridDim.x;
+        Chunk cnn;
+        if (wnn < nwork) cnn = chunk_of<E>(a, wnn, nchunk);
+        issue_chunk<N>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, wnn < nwork ? &cnn : nullptr, sPat);
+      }
+    }
+    // ---- interleaved own wavefield for the volume loop ------------------------------
+    if (!PML && active) {
+      float* dst = sQI + le * O::QE + n * QS;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) dst[c] = sQF[c * (E * Np) + le * Np + n];
+    }
     // ---- face amplitudes and expansion coefficients -----------------------------
     for (int i = tid; i < ne * NF; i += blockDim.x) {
       const int ee = i / NF, j = i - ee * NF;
       const int f = j / NpF, fi = j - f * NpF;
-      const int e = e0 + ee;
       const float* g = sGeo + ee * GEO_STRIDE;
-      const int code = reinterpret_cast<const int*>(a.fcode)[4 * e + f];
-      // own face node: fmask(fi, f) is pattern row 4*f+? -> stored as pattern id of the identity map
-      const int own = a.patterns[(size_t)f * NpF + fi];  // patterns 0..3 are the element's own face masks
-      const float* qo = sQ + (ee * Np + own) * QS;
+      const int code = sIds[ee * 12 + 8 + f];
+      const int own = sPat[f * NpF + fi];  // patterns 0..3 are the element's own face masks
+      const float* qo = sQF + ee * Np + own;
       float dq[9];
       bool free_face = false;
       if (code >= 0) {
-        const int nb = reinterpret_cast<const int*>(a.nbr)[4 * e + f];
-        const int nn = a.patterns[(size_t)code * NpF + fi];
-        const long long gn = (long long)nb * Np + nn;
+        const float* tr = sTr + i * 9;
 #pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = __ldg(qin + c * a.ldq + gn) - qo[c];
+        for (int c = 0; c < 9; ++c) dq[c] = tr[c] - qo[c * (E * Np)];
       } else if (code == -1) {
 #pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = qo[c];
+        for (int c = 0; c < 9; ++c) dq[c] = qo[c * (E * Np)];
         free_face = true;
       } else {
 #pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = -qo[c];
+        for (int c = 0; c < 9; ++c) dq[c] = -qo[c * (E * Np)];
       }
       float ap, as1, as2;
       face_amplitudes(g, f, dq, free_face, ap, as1, as2);
       const float fs = g[G_FS + f];
-      *reinterpret_cast<float4*>(sAmp + (ee * NF + j) * 4) = make_float4(ap * fs, as1 * fs, as2 * fs, 0.f);
+      float* am = sAmp + ee * O::AE + f * 2 * O::NPAIR + fi;
+      am[0] = ap * fs;
+      am[O::NFP] = as1 * fs;
+      am[2 * O::NFP] = as2 * fs;
     }
     for (int i = tid; i < ne * 4; i += blockDim.x) face_coeffs(sGeo + (i >> 2) * GEO_STRIDE, i & 3, sG + i * GS);
 
     // ---- PML: auxiliary update and contravariant modified fluxes ------------------
     float vgrad[9];  // d(v_c)/d(x_d) [c*3+d] (anelastic)
     (void)vgrad;
-    if (PML) {
-      if (le < ne) {
-        const int e = e0 + le;
-        const float* g = sGeo + le * GEO_STRIDE;
-        const float* qn_ = sQ + (le * Np + n) * QS;
-        float F[9], G[9], H[9];
-        const float e1 = g[G_E1], e2 = g[G_E2], e3 = g[G_E3], e4 = g[G_E4];
-        F[0] = e1 * qn_[6]; F[1] = e2 * qn_[6]; F[2] = e2 * qn_[6]; F[3] = e3 * qn_[7]; F[4] = 0.f;
-        F[5] = e3 * qn_[8]; F[6] = e4 * qn_[0]; F[7] = e4 * qn_[3]; F[8] = e4 * qn_[5];
-        G[0] = e2 * qn_[7]; G[1] = e1 * qn_[7]; G[2] = e2 * qn_[7]; G[3] = e3 * qn_[6]; G[4] = e3 * qn_[8];
-        G[5] = 0.f; G[6] = e4 * qn_[3]; G[7] = e4 * qn_[1]; G[8] = e4 * qn_[4];
-        H[0] = e2 * qn_[8]; H[1] = e2 * qn_[8]; H[2] = e1 * qn_[8]; H[3] = 0.f; H[4] = e3 * qn_[7];
-        H[5] = e3 * qn_[6]; H[6] = e4 * qn_[5]; H[7] = e4 * qn_[4]; H[8] = e4 * qn_[2];
-        const int slot = e;  // PML elements come first in the internal order
-        const long long pn = (long long)slot * Np + n;
-        const float* pr = a.prof + (long long)slot * 9 * Np + n;
-        const float ddx = pr[0], ddy = pr[Np], ddz = pr[2 * Np];
-        const float alx = pr[3 * Np], aly = pr[4 * Np], alz = pr[5 * Np];
-        const float kx = pr[6 * Np], ky = pr[7 * Np], kz = pr[8 * Np];
-        const float ikx = 1.f / kx, iky = 1.f / ky, ikz = 1.f / kz;
-        float* aux = a.aux + (long long)b * 27 * a.lda + pn;
-        float* aux2 = a.aux2 + (long long)b * 27 * a.lda + pn;
-        float* cf = sCF + (le * Np + n) * CS;
+    if (PML && active) {
+      const int e = e0 + le;
+      const float* g = sGeo + le * GEO_STRIDE;
+      float qv[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-          const float fp = aux[i * a.lda], gp = aux[(9 + i) * a.lda], hp = aux[(18 + i) * a.lda];
-          const float rf = -alx * fp - ddx * ikx * (fp + F[i]);
-          const float rg = -aly * gp - ddy * iky * (gp + G[i]);
-          const float rh = -alz * hp - ddz * ikz * (hp + H[i]);
-          const float phi = (fp + F[i]) * ikx, psi = (gp + G[i]) * iky, ome = (hp + H[i]) * ikz;
-          cf[i] = g[G_RX] * phi + g[G_RY] * psi + g[G_RZ] * ome;
-          cf[9 + i] = g[G_SX] * phi + g[G_SY] * psi + g[G_SZ] * ome;
-          cf[18 + i] = g[G_TX] * phi + g[G_TY] * psi + g[G_TZ] * ome;
-          float nf, ng_, nh;
-          if (MODE == MODE_LSERK) {
-            const float r1 = a.ca * aux2[i * a.lda] + a.dt * rf;
-            const float r2 = a.ca * aux2[(9 + i) * a.lda] + a.dt * rg;
-            const float r3 = a.ca * aux2[(18 + i) * a.lda] + a.dt * rh;
-            aux2[i * a.lda] = r1;
-            aux2[(9 + i) * a.lda] = r2;
-            aux2[(18 + i) * a.lda] = r3;
-            nf = fp + a.cb * r1;
-            ng_ = gp + a.cb * r2;
-            nh = hp + a.cb * r3;
+      for (int c = 0; c < 9; ++c) qv[c] = sQF[c * (E * Np) + le * Np + n];
+      float F[9], G[9], H[9];
+      const float e1 = g[G_E1], e2 = g[G_E2], e3 = g[G_E3], e4 = g[G_E4];
+      F[0] = e1 * qv[6]; F[1] = e2 * qv[6]; F[2] = e2 * qv[6]; F[3] = e3 * qv[7]; F[4] = 0.f;
+      F[5] = e3 * qv[8]; F[6] = e4 * qv[0]; F[7] = e4 * qv[3]; F[8] = e4 * qv[5];
+      G[0] = e2 * qv[7]; G[1] = e1 * qv[7]; G[2] = e2 * qv[7]; G[3] = e3 * qv[6]; G[4] = e3 * qv[8];
+      G[5] = 0.f; G[6] = e4 * qv[3]; G[7] = e4 * qv[1]; G[8] = e4 * qv[4];
+      H[0] = e2 * qv[8]; H[1] = e2 * qv[8]; H[2] = e1 * qv[8]; H[3] = 0.f; H[4] = e3 * qv[7];
+      H[5] = e3 * qv[6]; H[6] = e4 * qv[5]; H[7] = e4 * qv[4]; H[8] = e4 * qv[2];
+      const long long pn = (long long)e * Np + n;  // PML elements come first in the internal order
+      const float ddx = pre_pr[0], ddy = pre_pr[1], ddz = pre_pr[2];
+      const float alx = pre_pr[3], aly = pre_pr[4], alz = pre_pr[5];
+      const float ikx = 1.f / pre_pr[6], iky = 1.f / pre_pr[7], ikz = 1.f / pre_pr[8];
+      float* aux = a.aux + (long long)b * 27 * a.lda + pn;
+      float* aux2 = a.aux2 + (long long)b * 27 * a.lda + pn;
+      float* cf = sCF + le * O::CFE + n * CS;
+      const float* av = pre_ax;
+      const float* a2 = pre_ax2;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        const float fp = av[i], gp = av[9 + i], hp = av[18 + i];
+        const float rf = -alx * fp - ddx * ikx * (fp + F[i]);
+        const float rg = -aly * gp - ddy * iky * (gp + G[i]);
+        const float rh = -alz * hp - ddz * ikz * (hp + H[i]);
+        const float phi = (fp + F[i]) * ikx, psi = (gp + G[i]) * iky, ome = (hp + H[i]) * ikz;
+        cf[i] = g[G_RX] * phi + g[G_RY] * psi + g[G_RZ] * ome;
+        cf[10 + i] = g[G_SX] * phi + g[G_SY] * psi + g[G_SZ] * ome;
+        cf[20 + i] = g[G_TX] * phi + g[G_TY] * psi + g[G_TZ] * ome;
+        float nf, ng_, nh;
+        if (MODE == MODE_LSERK) {
+          const float r1 = a.ca * a2[i] + a.dt * rf;
+          const float r2 = a.ca * a2[9 + i] + a.dt * rg;
+          const float r3 = a.ca * a2[18 + i] + a.dt * rh;
+          __stcs(aux2 + i * a.lda, r1);
+          __stcs(aux2 + (9 + i) * a.lda, r2);
+          __stcs(aux2 + (18 + i) * a.lda, r3);
+          nf = fp + a.cb * r1;
+          ng_ = gp + a.cb * r2;
+          nh = hp + a.cb * r3;
+        } else {
+          float n1, n2, n3;
+          if (a.stage_first) {
+            __stcs(aux2 + i * a.lda, fp);
+            __stcs(aux2 + (9 + i) * a.lda, gp);
+            __stcs(aux2 + (18 + i) * a.lda, hp);
+            n1 = fp; n2 = gp; n3 = hp;
           } else {
-            float n1, n2, n3;
-            if (a.stage_first) {
-              aux2[i * a.lda] = fp;
-              aux2[(9 + i) * a.lda] = gp;
-              aux2[(18 + i) * a.lda] = hp;
-              n1 = fp; n2 = gp; n3 = hp;
-            } else {
-              n1 = aux2[i * a.lda]; n2 = aux2[(9 + i) * a.lda]; n3 = aux2[(18 + i) * a.lda];
-            }
-            nf = a.ca * n1 + a.cb * (fp + a.dt * rf);
-            ng_ = a.ca * n2 + a.cb * (gp + a.dt * rg);
-            nh = a.ca * n3 + a.cb * (hp + a.dt * rh);
+            n1 = a2[i]; n2 = a2[9 + i]; n3 = a2[18 + i];
           }
-          aux[i * a.lda] = nf;
-          aux[(9 + i) * a.lda] = ng_;
-          aux[(18 + i) * a.lda] = nh;
+          nf = a.ca * n1 + a.cb * (fp + a.dt * rf);
+          ng_ = a.ca * n2 + a.cb * (gp + a.dt * rg);
+          nh = a.ca * n3 + a.cb * (hp + a.dt * rh);
         }
+        __stcs(aux + i * a.lda, nf);
+        __stcs(aux + (9 + i) * a.lda, ng_);
+        __stcs(aux + (18 + i) * a.lda, nh);
       }
     }
     __syncthreads();
-    if (le >= ne) continue;  // idle threads of a partial chunk (no barrier follows in this iteration)
+    if (!active) continue;  // idle threads of a partial chunk (the next barrier is at the loop top)
 
     const int e = e0 + le;
     const float* g = sGeo + le * GEO_STRIDE;
     float rq[9];
     // ---- volume term ------------------------------------------------------------
     if (!PML) {
-      float dr[9], ds[9], dtt[9];
+      // d/dr, d/ds, d/dt of the 9 fields as packed pairs (fields 2j, 2j+1; pair 4 = field 8 + pad)
+      float2 ar[5], as_[5], at[5];
 #pragma unroll
-      for (int c = 0; c < 9; ++c) { dr[c] = 0.f; ds[c] = 0.f; dtt[c] = 0.f; }
-      const float* qe = sQ + le * Np * QS;
+      for (int j = 0; j < 5; ++j) { ar[j] = make_float2(0.f, 0.f); as_[j] = ar[j]; at[j] = ar[j]; }
+      const float* qe = sQI + le * O::QE;
 #pragma unroll 5
       for (int k = 0; k < Np; ++k) {
-        const float d0 = sD[k * Np + n], d1 = sD[Np * Np + k * Np + n], d2 = sD[2 * Np * Np + k * Np + n];
+        const float dx = sD[k * Np + n], dy = sD[Np * Np + k * Np + n], dz = sD[2 * Np * Np + k * Np + n];
+        const float2 d0 = make_float2(dx, dx), d1 = make_float2(dy, dy), d2 = make_float2(dz, dz);
         const float4 qa = ld4(qe + k * QS), qb = ld4(qe + k * QS + 4);
-        const float q8 = qe[k * QS + 8];
-        const float qq[9] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w, q8};
+        const float2 qc = *reinterpret_cast<const float2*>(qe + k * QS + 8);
+        const float2 qp[5] = {make_float2(qa.x, qa.y), make_float2(qa.z, qa.w), make_float2(qb.x, qb.y),
+                              make_float2(qb.z, qb.w), qc};
 #pragma unroll
-        for (int c = 0; c < 9; ++c) {
-          dr[c] = fmaf(d0, qq[c], dr[c]);
-          ds[c] = fmaf(d1, qq[c], ds[c]);
-          dtt[c] = fmaf(d2, qq[c], dtt[c]);
+        for (int j = 0; j < 5; ++j) {
+          ar[j] = __ffma2_rn(d0, qp[j], ar[j]);
+          as_[j] = __ffma2_rn(d1, qp[j], as_[j]);
+          at[j] = __ffma2_rn(d2, qp[j], at[j]);
         }
       }
+      float dr[9], ds[9], dtt[9];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        dr[2 * j] = ar[j].x; dr[2 * j + 1] = ar[j].y;
+        ds[2 * j] = as_[j].x; ds[2 * j + 1] = as_[j].y;
+        dtt[2 * j] = at[j].x; dtt[2 * j + 1] = at[j].y;
+      }
+      dr[8] = ar[4].x; ds[8] = as_[4].x; dtt[8] = at[4].x;
       const float rx = g[G_RX], ry = g[G_RY], rz = g[G_RZ], sx = g[G_SX], sy = g[G_SY], sz = g[G_SZ],
                   tx = g[G_TX], ty = g[G_TY], tz = g[G_TZ];
 #define DX(c) (rx * dr[c] + sx * ds[c] + tx * dtt[c])
@@ -373,25 +559,35 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     } else {
 #pragma unroll
       for (int c = 0; c < 9; ++c) rq[c] = 0.f;
-      float vr[3] = {0.f, 0.f, 0.f}, vs3[3] = {0.f, 0.f, 0.f}, vt3[3] = {0.f, 0.f, 0.f};
-      const float* cfe = sCF + le * Np * CS;
-      const float* qe = sQ + le * Np * QS;
+      float2 acc[5];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) acc[j] = make_float2(0.f, 0.f);
+      float2 v01r = make_float2(0.f, 0.f), v01s = v01r, v01t = v01r;
+      float v2r = 0.f, v2s = 0.f, v2t = 0.f;
+      const float* cfe = sCF + le * O::CFE;
+      const float* qv = sQF + le * Np;
 #pragma unroll 2
       for (int k = 0; k < Np; ++k) {
-        const float d0 = sD[k * Np + n], d1 = sD[Np * Np + k * Np + n], d2 = sD[2 * Np * Np + k * Np + n];
-        const float* cf = cfe + k * CS;
+        const float4 d = make_float4(sD[k * Np + n], sD[Np * Np + k * Np + n], sD[2 * Np * Np + k * Np + n], 0.f);
+        const float2 d0 = make_float2(d.x, d.x), d1 = make_float2(d.y, d.y), d2 = make_float2(d.z, d.z);
+        const float2* cf = reinterpret_cast<const float2*>(cfe + k * CS);
 #pragma unroll
-        for (int c = 0; c < 9; ++c) rq[c] = fmaf(d0, cf[c], fmaf(d1, cf[9 + c], fmaf(d2, cf[18 + c], rq[c])));
+        for (int j = 0; j < 5; ++j) acc[j] = __ffma2_rn(d0, cf[j], __ffma2_rn(d1, cf[5 + j], __ffma2_rn(d2, cf[10 + j], acc[j])));
         if (ATT) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const float v = qe[k * QS + 6 + c];
-            vr[c] = fmaf(d0, v, vr[c]);
-            vs3[c] = fmaf(d1, v, vs3[c]);
-            vt3[c] = fmaf(d2, v, vt3[c]);
-          }
+          const float2 v01 = make_float2(qv[6 * (E * Np) + k], qv[7 * (E * Np) + k]);
+          const float v2 = qv[8 * (E * Np) + k];
+          v01r = __ffma2_rn(d0, v01, v01r);
+          v01s = __ffma2_rn(d1, v01, v01s);
+          v01t = __ffma2_rn(d2, v01, v01t);
+          v2r = fmaf(d.x, v2, v2r);
+          v2s = fmaf(d.y, v2, v2s);
+          v2t = fmaf(d.z, v2, v2t);
         }
       }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) { rq[2 * j] = acc[j].x; rq[2 * j + 1] = acc[j].y; }
+      rq[8] = acc[4].x;
+      const float vr[3] = {v01r.x, v01r.y, v2r}, vs3[3] = {v01s.x, v01s.y, v2s}, vt3[3] = {v01t.x, v01t.y, v2t};
       if (ATT) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -408,18 +604,21 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     (void)sig_an;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-      float A0 = 0.f, A1 = 0.f, A2 = 0.f;
-      const float* am = sAmp + (le * NF + f * NpF) * 4;
-      const float* lf = sL + f * NpF * Np + n;
-#pragma unroll 5
-      for (int i = 0; i < NpF; ++i) {
-        const float l = lf[i * Np];
-        const float4 v = ld4(am + i * 4);
-        A0 = fmaf(l, v.x, A0);
-        A1 = fmaf(l, v.y, A1);
-        A2 = fmaf(l, v.z, A2);
+      float2 c0 = make_float2(0.f, 0.f), c1 = c0, c2 = c0;
+      const float2* lp = reinterpret_cast<const float2*>(sL) + f * O::NPAIR * Np + n;
+      const float* ax = sAmp + le * O::AE + f * 2 * O::NPAIR;
+#pragma unroll
+      for (int ip = 0; ip < O::NPAIR; ++ip) {
+        const float2 l = lp[ip * Np];
+        c0 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + 2 * ip), c0);
+        c1 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + O::NFP + 2 * ip), c1);
+        c2 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + 2 * O::NFP + 2 * ip), c2);
       }
-      const float* G = sG + (le * 4 + f) * GS;
+      const float A0 = c0.x + c0.y, A1 = c1.x + c1.y, A2 = c2.x + c2.y;
+      const float4* G4 = reinterpret_cast<const float4*>(sG + (le * 4 + f) * GS);
+      const float4 g0 = G4[0], g1 = G4[1], g2 = G4[2], g3 = G4[3], g4 = G4[4], g5 = G4[5], g6 = G4[6];
+      const float G[28] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w, g2.x, g2.y, g2.z, g2.w, g3.x, g3.y,
+                           g3.z, g3.w, g4.x, g4.y, g4.z, g4.w, g5.x, g5.y, g5.z, g5.w, g6.x, g6.y, g6.z, g6.w};
       float X[6];
 #pragma unroll
       for (int c = 0; c < 6; ++c) X[c] = G[6 + c] * A1 + G[12 + c] * A2;
@@ -430,11 +629,12 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
       rq[8] += G[20] * A0 + G[23] * A1 + G[26] * A2;
       if (ATT) {
         const float as = g[G_AS];
+        const float4 g7 = G4[7], g8 = G4[8];
+        const float NN[6] = {G[27], g7.x, g7.y, g7.z, g7.w, g8.x};
 #pragma unroll
-        for (int c = 0; c < 6; ++c) sig_an[c] += G[27 + c] * A0 + X[c] * as;
+        for (int c = 0; c < 6; ++c) sig_an[c] += NN[c] * A0 + X[c] * as;
       }
     }
-    const long long node = (long long)e * Np + n;
     // ---- Zener memory variables (src/timeloopMod.f90:426-461) ------------------
     if (ATT) {
       // S = -strain rate + lifted anelastic flux; d theta_l/dt = w_l (S - theta_l)
@@ -445,14 +645,14 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
       S[3] = sig_an[3] - 0.5f * (vgrad[3] + vgrad[1]);
       S[4] = sig_an[4] - 0.5f * (vgrad[7] + vgrad[5]);
       S[5] = sig_an[5] - 0.5f * (vgrad[6] + vgrad[2]);
-      float* th = a.th + (long long)b * 6 * a.nMB * a.ldt + node;
-      float* th2 = a.th2 + (long long)b * 6 * a.nMB * a.ldt + node;
-      const float* ae = a.ael + (long long)e * 3 * a.nMB;
-      for (int l = 0; l < a.nMB; ++l) {
-        const float wl = a.wl[l];
-        float t[6];
+      float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
+      float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
+      const float* ae = a.ael + (long long)e * 3 * kNMB;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) t[j] = th[(l * 6 + j) * a.ldt];
+      for (int l = 0; l < kNMB; ++l) {
+        const float wl = a.wl[l];
+        const float* t = pre_th + 6 * l;
+        const float* t2 = pre_th2 + 6 * l;
         const float c1 = ae[3 * l], c2 = ae[3 * l + 1], c3 = ae[3 * l + 2];
         rq[0] += c3 * t[0] + c1 * (t[1] + t[2]);
         rq[1] += c3 * t[1] + c1 * (t[2] + t[0]);
@@ -466,15 +666,15 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
           const long long o = (l * 6 + j) * a.ldt;
           float nt_;
           if (MODE == MODE_LSERK) {
-            const float rr = a.ca * th2[o] + a.dt * r;
-            th2[o] = rr;
+            const float rr = a.ca * t2[j] + a.dt * r;
+            __stcs(th2 + o, rr);
             nt_ = t[j] + a.cb * rr;
           } else {
             float tn;
-            if (a.stage_first) { th2[o] = t[j]; tn = t[j]; } else { tn = th2[o]; }
+            if (a.stage_first) { __stcs(th2 + o, t[j]); tn = t[j]; } else { tn = t2[j]; }
             nt_ = a.ca * tn + a.cb * (t[j] + a.dt * r);
           }
-          th[o] = nt_;
+          __stcs(th + o, nt_);
         }
       }
     }
@@ -498,25 +698,25 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
       }
     }
     // ---- stage update ------------------------------------------------------------
-    const float* qown = sQ + (le * Np + n) * QS;
     float* qo = a.q_out + (long long)b * 9 * a.ldq + node;
+    const float* qown = sQF + le * Np + n;
     if (MODE == MODE_LSERK) {
       float* rs = a.res + (long long)b * 9 * a.ldq + node;
 #pragma unroll
       for (int c = 0; c < 9; ++c) {
-        const float r = a.ca * rs[c * a.ldq] + a.dt * rq[c];
-        rs[c * a.ldq] = r;
-        qo[c * a.ldq] = qown[c] + a.cb * r;
+        const float r = a.ca * pre_res[c] + a.dt * rq[c];
+        __stcs(rs + c * a.ldq, r);
+        __stcs(qo + c * a.ldq, qown[c * (E * Np)] + a.cb * r);
       }
     } else {
-      const float* qn = a.q_n + (long long)b * 9 * a.ldq + node;
 #pragma unroll
       for (int c = 0; c < 9; ++c) {
-        const float base = (a.ca != 0.f) ? a.ca * qn[c * a.ldq] : 0.f;
-        qo[c * a.ldq] = base + a.cb * (qown[c] + a.dt * rq[c]);
+        const float base = (a.ca != 0.f) ? a.ca * pre_res[c] : 0.f;
+        __stcs(qo + c * a.ldq, base + a.cb * (qown[c * (E * Np)] + a.dt * rq[c]));
       }
     }
   }
+  cp_async_wait_all();
 }
 
 // Receiver gather: one warp per (batch, receiver) (src/timeloopMod.f90:358-373).

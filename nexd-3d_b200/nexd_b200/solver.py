@@ -45,18 +45,47 @@ class Solver:
             raise _gpu_error(self._ctx, st)
         return out
 
-    def field(self, b=0):
-        out = np.zeros((self.K * self.Np, 9), dtype=np.float32, order="F")
-        st = _abi.gpu_lib().nexd_get_field(self._ctx, b, out.ctypes.data_as(C.POINTER(C.c_float)))
+    def state(self, which=_abi.NEXD_STATE_Q, b=0, nfields=9):
+        """Copy of a state array: q (K*Np,9), theta (K*Np,6*nMB) or PML
+        auxiliaries (K*Np,27)."""
+        out = np.zeros((self.K * self.Np, nfields), dtype=np.float32, order="F")
+        st = _abi.gpu_lib().nexd_get_state(self._ctx, which, b, out.ctypes.data_as(C.POINTER(C.c_float)))
         if st != 0:
             raise _gpu_error(self._ctx, st)
         return out
 
-    def set_field(self, q, b=0):
-        q = np.asfortranarray(q, dtype=np.float32)
-        st = _abi.gpu_lib().nexd_set_field(self._ctx, b, q.ctypes.data_as(C.POINTER(C.c_float)))
+    def set_state(self, arr, which=_abi.NEXD_STATE_Q, b=0):
+        arr = np.asfortranarray(arr, dtype=np.float32)
+        st = _abi.gpu_lib().nexd_set_state(self._ctx, which, b, arr.ctypes.data_as(C.POINTER(C.c_float)))
         if st != 0:
             raise _gpu_error(self._ctx, st)
+
+    def field(self, b=0):
+        return self.state(_abi.NEXD_STATE_Q, b, 9)
+
+    def set_field(self, q, b=0):
+        self.set_state(q, _abi.NEXD_STATE_Q, b)
+
+    def step_io(self, it, stf_in, traces_out):
+        """One step with host source samples in and that step's receiver samples out."""
+        sp = None if stf_in is None else stf_in.ctypes.data_as(C.POINTER(C.c_float))
+        st = _abi.gpu_lib().nexd_step_io(self._ctx, it, sp, traces_out.ctypes.data_as(C.POINTER(C.c_float)))
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+
+    def profile(self, enable=None):
+        """Enable/disable CUDA-event timing (enable=True/False) or return the
+        per-kernel-kind counters as a dict."""
+        lib = _abi.gpu_lib()
+        if enable is not None:
+            lib.nexd_profile_enable(self._ctx, 1 if enable else 0)
+            return None
+        p = _abi.NexdProfile()
+        lib.nexd_profile_get(self._ctx, C.byref(p))
+        names = ("record", "stage_pml", "stage_main")
+        out = {n: dict(launches=p.launches[i], ms=p.ms[i], elements=p.elements[i]) for i, n in enumerate(names)}
+        out["span_ms"] = p.span_ms
+        return out
 
     def launch_count(self):
         n = C.c_int64()

@@ -190,14 +190,14 @@ def write_cube(directory, *, cells=10, seed=1, nt=1000):
 
 
 def write_twolayer(directory, *, cells=(40, 40, 20), seed=2, nt=3000, nrec=100, nsrc=1, attenuation=True,
-                   pml=True, f0=3.0, src_depth=(1500.0, 1500.0), f0_range=None):
+                   pml=True, f0=3.0, src_depth=(1500.0, 1500.0), f0_range=None, src_seed=None):
     """Two-layer anelastic box 4x4x2 km (40x40x20 hexahedra x 6 = 192,000 tets):
     upper 600 m vp 3000 / vs 1730 / rho 2400 / Qp 100 / Qs 50, half-space 5000 /
     2890 / 2800 / 400 / 200; 3-cell NPML on the sides and bottom, free top;
     seeded double-couple sources (Ricker), random surface receivers."""
     Lx, Ly, Lz = 4000.0, 4000.0, 2000.0
     nx, ny, nz = cells
-    rng = np.random.default_rng(seed)
+    rng = np.random.default_rng(seed if src_seed is None else src_seed)
     hx = Lx / nx
     margin = min(4 * hx, 0.25 * Lx)
     srcs = []

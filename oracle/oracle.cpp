@@ -583,12 +583,21 @@ int run_t(const nexd_desc* d, int it_end, float* traces, double* field) {
 }
 
 template <class R>
-int rhs_t(const nexd_desc* d, int it, int stage, const double* q, double* rq) {
+int rhs_t(const nexd_desc* d, int it, int stage, const double* q, const double* theta, const double* aux,
+          double* rq, double* arq, double* auxr) {
   Oracle<R> o(*d);
   o.alloc();
   for (size_t i = 0; i < o.ng * 9; ++i) o.q[i] = R(q[i]);
+  if (o.att && theta)
+    for (size_t i = 0; i < o.th.size(); ++i) o.th[i] = R(theta[i]);
+  if (o.pml && aux)
+    for (size_t i = 0; i < o.aux.size(); ++i) o.aux[i] = R(aux[i]);
   o.rhs_all(o.q, o.att ? &o.th : nullptr, o.pml ? &o.aux : nullptr, it, stage, 0);
   for (size_t i = 0; i < o.ng * 9; ++i) rq[i] = double(o.rq[i]);
+  if (arq && o.att)
+    for (size_t i = 0; i < o.arq.size(); ++i) arq[i] = double(o.arq[i]);
+  if (auxr && o.pml)
+    for (size_t i = 0; i < o.auxr.size(); ++i) auxr[i] = double(o.auxr[i]);
   return 0;
 }
 
@@ -620,10 +629,12 @@ int oracle_run(const nexd_desc* d, int precision, int it_end, float* traces, dou
   }
 }
 
-int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const double* q, double* rq) {
+int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const double* q, const double* theta,
+               const double* aux, double* rq, double* arq, double* auxr) {
   if (!check_desc(d) || !q || !rq) return NEXD_ERR_INVALID;
   try {
-    return precision == 32 ? rhs_t<float>(d, it, stage, q, rq) : rhs_t<double>(d, it, stage, q, rq);
+    return precision == 32 ? rhs_t<float>(d, it, stage, q, theta, aux, rq, arq, auxr)
+                           : rhs_t<double>(d, it, stage, q, theta, aux, rq, arq, auxr);
   } catch (const std::exception& e) {
     g_err = e.what();
     return NEXD_ERR_INVALID;

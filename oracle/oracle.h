@@ -27,10 +27,13 @@ extern "C" {
  * code (message via oracle_last_error). */
 int oracle_run(const nexd_desc* d, int precision, int it_end, float* traces, double* field, int nthreads);
 
-/* One right-hand side evaluation rq = L(q) for batch member 0 at step `it`
- * (1-based) and stage `stage` (0-based), with q given as (K*Np,9) FP64 and
- * the anelastic / PML auxiliaries set to `aux_value`.  rq out: (K*Np,9). */
-int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const double* q, double* rq);
+/* One right-hand side evaluation for batch member 0 at step `it` (1-based)
+ * and stage `stage` (0-based).  Inputs (FP64): q (K*Np,9); theta
+ * (K*Np,6*nMB) or NULL (start value); aux (K*Np,27) or NULL (zero).  Outputs:
+ * rq (K*Np,9); arq (K*Np,6*nMB) or NULL; auxr (K*Np,27) or NULL (zero outside
+ * PML elements). */
+int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const double* q, const double* theta,
+               const double* aux, double* rq, double* arq, double* auxr);
 
 int oracle_last_error(char* buf, size_t len);
 

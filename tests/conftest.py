@@ -46,7 +46,7 @@ def oracle(built):
     lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
     lib.oracle_run.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_void_p, C.c_int]
     lib.oracle_run.restype = C.c_int
-    lib.oracle_rhs.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    lib.oracle_rhs.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 6
     lib.oracle_rhs.restype = C.c_int
     return lib
 
@@ -121,14 +121,19 @@ def rel_l2(a, b):
 
 
 def trace_misfit(test, ref):
-    """Relative L2 per receiver and kind (u, v, a), normalised by the norm of
-    all three components of that kind; returns the maximum."""
+    """Relative L2 of the receiver traces, per trace kind (u, v, a) over all
+    receivers and components; returns the largest of the three."""
+    return max(rel_l2(test[:, :, 3 * k:3 * k + 3], ref[:, :, 3 * k:3 * k + 3]) for k in range(3))
+
+
+def station_misfit(test, ref):
+    """Relative L2 per receiver and kind, normalised by that receiver's three
+    components of the kind; returns the maximum (meaningful only when every
+    receiver has recorded the wave)."""
     worst = 0.0
     for r in range(ref.shape[0]):
         for k in range(3):
-            g = ref[r, :, 3 * k:3 * k + 3]
-            o = test[r, :, 3 * k:3 * k + 3]
-            worst = max(worst, rel_l2(o, g))
+            worst = max(worst, rel_l2(test[r, :, 3 * k:3 * k + 3], ref[r, :, 3 * k:3 * k + 3]))
     return worst
 
 
