@@ -170,8 +170,33 @@ int nexd_set_state(nexd_ctx* ctx, int32_t which, int32_t b, const float* in);
  * it.  Host buffers are staged through pinned memory owned by the context. */
 int nexd_step_io(nexd_ctx* ctx, int32_t it, const float* stf_in, float* traces_out);
 
+/* Arms the reference's NPML stability trigger (src/timeloopMod.f90:508-542):
+ * after every step the wavefield energy
+ *   E = sum_e 1/2 J_e [rho v^T M v + sum_{i<=3} q_i^T M e_i + 2 sum_{i>3} q_i^T M e_i]
+ * is reduced on the device (FP64); once it > 2.4/(f0 dt), the ratio of the
+ * mean over the last avg_window2 steps to the mean over the last avg_window1
+ * steps is tested against sta_lta_trigger and, when |ratio - 1| exceeds it,
+ * the NPML of that wavefield is switched off for the rest of the run
+ * (pmlcheck(:) = .false.).  formula 0 evaluates the strain e exactly as the
+ * reference does (src/timeloopMod.f90:493-500, including e3 from q1+q1 and the
+ * division by 1/(4mu^2+6mu*lambda)); formula 1 uses the isotropic compliance.
+ * f0: the largest source centre frequency.  Requires set_pml. */
+int nexd_pml_trigger(nexd_ctx* ctx, int32_t avg_window1, int32_t avg_window2, double sta_lta_trigger, double f0,
+                     int32_t formula);
+
+/* Energy history (nt, nbatch) of the steps run since nexd_pml_trigger (0
+ * elsewhere) and, per wavefield, the step at which the NPML was switched off
+ * (0 = never), the `pmlswitch` of the reference. */
+int nexd_get_energy(nexd_ctx* ctx, double* energy, int32_t* pml_switch);
+
 /* Kernel kinds reported by nexd_profile_get. */
-enum nexd_kernel_kind { NEXD_K_RECORD = 0, NEXD_K_STAGE_PML = 1, NEXD_K_STAGE_MAIN = 2, NEXD_K_COUNT = 3 };
+enum nexd_kernel_kind {
+  NEXD_K_RECORD = 0,
+  NEXD_K_STAGE_PML = 1,
+  NEXD_K_STAGE_MAIN = 2,
+  NEXD_K_ENERGY = 3,
+  NEXD_K_COUNT = 4
+};
 
 typedef struct nexd_profile {
   int64_t launches[NEXD_K_COUNT]; /* launches per kernel kind since profiling was enabled */

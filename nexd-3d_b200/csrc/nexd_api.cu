@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/nexd.h"
+#include "energy_kernel.cuh"
 #include "stage_kernel.cuh"
 
 using namespace nexd_dev;
@@ -76,6 +77,17 @@ struct nexd_ctx {
   // pinned staging for nexd_step_io
   float* pinned = nullptr;
   size_t pinned_floats = 0;
+  // NPML energy / STA-LTA trigger
+  int* pml_off = nullptr;     // [nbatch]
+  int* pml_switch = nullptr;  // [nbatch]
+  bool energy_on = false;
+  int trig_w1 = 10, trig_w2 = 2, trig_timecrit = 0, trig_formula = 0;
+  float trig_threshold = 0.1f;
+  double* energy = nullptr;    // [nbatch][nt]
+  double* partials = nullptr;  // [nbatch][energy_blocks]
+  float4* emat = nullptr;      // [K] (rho, lambda, mu, J)
+  double* mass = nullptr;      // [Np][Np]
+  int energy_blocks = 0;
 };
 
 namespace {
@@ -473,6 +485,44 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     CUDA_TRY(c, cudaMemset(c->traces, 0, nt_ * sizeof(float)));
     if ((st = dalloc(c, &c->flag, 1))) return fail(st);
     CUDA_TRY(c, cudaMemset(c->flag, 0, sizeof(int)));
+    if ((st = dalloc(c, &c->pml_off, size_t(nb))) || (st = dalloc(c, &c->pml_switch, size_t(nb)))) return fail(st);
+    CUDA_TRY(c, cudaMemset(c->pml_off, 0, nb * sizeof(int)));
+    CUDA_TRY(c, cudaMemset(c->pml_switch, 0, nb * sizeof(int)));
+    // mass matrix M = (V V^T)^-1 and per-element energy constants, for the NPML trigger
+    if (c->pml) {
+      std::vector<double> Mi(d->invmass, d->invmass + size_t(Np) * Np), Mo(size_t(Np) * Np, 0.0);
+      for (int i = 0; i < Np; ++i) Mo[size_t(i) * Np + i] = 1.0;
+      for (int col = 0; col < Np; ++col) {  // Gauss-Jordan with partial pivoting
+        int p = col;
+        for (int r = col + 1; r < Np; ++r)
+          if (std::fabs(Mi[size_t(col) * Np + r]) > std::fabs(Mi[size_t(col) * Np + p])) p = r;
+        for (int j = 0; j < Np; ++j) {
+          std::swap(Mi[size_t(j) * Np + col], Mi[size_t(j) * Np + p]);
+          std::swap(Mo[size_t(j) * Np + col], Mo[size_t(j) * Np + p]);
+        }
+        const double piv = Mi[size_t(col) * Np + col];
+        if (piv == 0.0) return fail(set_err(c, NEXD_ERR_INVALID, "singular invmass"));
+        for (int j = 0; j < Np; ++j) { Mi[size_t(j) * Np + col] /= piv; Mo[size_t(j) * Np + col] /= piv; }
+        for (int r = 0; r < Np; ++r) {
+          if (r == col) continue;
+          const double f = Mi[size_t(col) * Np + r];
+          if (f == 0.0) continue;
+          for (int j = 0; j < Np; ++j) {
+            Mi[size_t(j) * Np + r] -= f * Mi[size_t(j) * Np + col];
+            Mo[size_t(j) * Np + r] -= f * Mo[size_t(j) * Np + col];
+          }
+        }
+      }
+      std::vector<double> h_mass(size_t(Np) * Np);  // row-major M(n,k)
+      for (int n = 0; n < Np; ++n)
+        for (int k = 0; k < Np; ++k) h_mass[size_t(n) * Np + k] = Mo[size_t(k) * Np + n];
+      std::vector<float4> h_emat(K);
+      for (int ni = 0; ni < K; ++ni) {
+        const int e = c->new2old[ni];
+        h_emat[ni] = make_float4(float(d->rho[e]), float(d->lambdau[e]), float(d->muu[e]), float(d->jacobian[e]));
+      }
+      if ((st = upload(c, &c->mass, h_mass)) || (st = upload(c, &c->emat, h_emat))) return fail(st);
+    }
   }
   // ---- launch configuration ----
   const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
@@ -567,6 +617,7 @@ void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
   a.rec_slot = c->rec_slot;
   a.abuf = c->abuf;
   a.nslot = std::max(1, c->nslot);
+  a.pml_off = c->pml_off;
   RecordArgs r{};
   r.nrec = c->nrec;
   r.nbatch = c->nbatch;
@@ -640,6 +691,39 @@ void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
       }
       if (c->timeint == 4 || c->timeint == 1) c->cur = outb;
     }
+    if (c->energy_on) {
+      // wavefield energy of step it and the STA/LTA rule (src/timeloopMod.f90:508-542)
+      EnergyArgs ea{};
+      ea.K = c->K;
+      ea.Np = c->Np;
+      ea.nbatch = c->nbatch;
+      ea.ldq = c->ldq;
+      ea.q = c->qbuf[c->cur];
+      ea.emat = c->emat;
+      ea.mass = c->mass;
+      ea.partials = c->partials;
+      ea.formula = c->trig_formula;
+      const int E = kEnergyThreads / c->Np;
+      const size_t smem = (size_t(c->Np) * c->Np + size_t(E) * 9 * c->Np) * sizeof(double);
+      const int ev = ev_begin(c, NEXD_K_ENERGY);
+      energy_kernel<<<dim3(c->energy_blocks, c->nbatch), kEnergyThreads, smem, c->stream>>>(ea);
+      TriggerArgs ta{};
+      ta.partials = c->partials;
+      ta.nparts = c->energy_blocks;
+      ta.energy = c->energy;
+      ta.nt = c->nt;
+      ta.it = it;
+      ta.armed = 1;
+      ta.timecrit = c->trig_timecrit;
+      ta.w1 = c->trig_w1;
+      ta.w2 = c->trig_w2;
+      ta.threshold = c->trig_threshold;
+      ta.pml_off = c->pml_off;
+      ta.pml_switch = c->pml_switch;
+      energy_finalize<<<c->nbatch, 256, 0, c->stream>>>(ta);
+      ev_end(c, ev);
+      c->launches += 2;
+    }
   }
 }
 
@@ -703,6 +787,49 @@ int nexd_step_io(nexd_ctx* c, int32_t it, const float* stf_in, float* traces_out
   int st = finish(c);
   if (st) return st;
   if (nout > 0) std::memcpy(traces_out, c->pinned + nin, nout * sizeof(float));
+  return NEXD_OK;
+}
+
+int nexd_pml_trigger(nexd_ctx* c, int32_t avg_window1, int32_t avg_window2, double sta_lta_trigger, double f0,
+                     int32_t formula) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (!c->pml) return set_err(c, NEXD_ERR_INVALID, "the STA/LTA trigger needs set_pml");
+  if (avg_window1 < 1 || avg_window2 < 1 || !(f0 > 0.0) || !(sta_lta_trigger >= 0.0) || (formula != 0 && formula != 1))
+    return set_err(c, NEXD_ERR_INVALID, "bad trigger parameters");
+  c->trig_w1 = avg_window1;
+  c->trig_w2 = avg_window2;
+  c->trig_threshold = float(sta_lta_trigger);
+  c->trig_formula = formula;
+  c->trig_timecrit = int(float(2.4 / f0 / c->dt));  // timecrit = 2.4/f0/deltat (integer)
+  if (!c->energy) {
+    c->energy_blocks = std::max(1, std::min(4 * c->nsm, (c->K + kEnergyThreads / c->Np - 1) / (kEnergyThreads / c->Np)));
+    int st;
+    if ((st = dalloc(c, &c->energy, size_t(c->nbatch) * c->nt)) ||
+        (st = dalloc(c, &c->partials, size_t(c->nbatch) * c->energy_blocks)))
+      return st;
+    const int E = kEnergyThreads / c->Np;
+    const size_t smem = (size_t(c->Np) * c->Np + size_t(E) * 9 * c->Np) * sizeof(double);
+    CUDA_TRY(c, cudaFuncSetAttribute(energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  }
+  CUDA_TRY(c, cudaMemsetAsync(c->energy, 0, size_t(c->nbatch) * c->nt * sizeof(double), c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->energy_on = true;
+  return NEXD_OK;
+}
+
+int nexd_get_energy(nexd_ctx* c, double* energy, int32_t* pml_switch) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (energy) {
+    if (!c->energy) {
+      std::fill(energy, energy + size_t(c->nbatch) * c->nt, 0.0);
+    } else {
+      CUDA_TRY(c, cudaMemcpyAsync(energy, c->energy, size_t(c->nbatch) * c->nt * sizeof(double),
+                                  cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
+  if (pml_switch)
+    CUDA_TRY(c, cudaMemcpyAsync(pml_switch, c->pml_switch, c->nbatch * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return NEXD_OK;
 }
 

@@ -134,6 +134,7 @@ struct StageArgs {
   float* abuf;           // [nbatch][nslot][3][Np]: last-stage rq(7:9)
   int nslot;
   int last_stage;
+  const int* pml_off;    // [nbatch] 1 once the STA/LTA trigger switched the NPML off
 };
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
@@ -454,6 +455,14 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       float* cf = sCF + le * O::CFE + n * CS;
       const float* av = pre_ax;
       const float* a2 = pre_ax2;
+      if (a.pml_off[b]) {  // pmlcheck(:) = .false.: ordinary element (src/timeloopMod.f90:537)
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+          cf[i] = g[G_RX] * F[i] + g[G_RY] * G[i] + g[G_RZ] * H[i];
+          cf[10 + i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
+          cf[20 + i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
+        }
+      } else
 #pragma unroll
       for (int i = 0; i < 9; ++i) {
         const float fp = av[i], gp = av[9 + i], hp = av[18 + i];

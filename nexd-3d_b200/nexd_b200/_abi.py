@@ -62,9 +62,10 @@ class NexdMeshInfo(C.Structure):
 HOST_SYMBOLS = ["nexd_mesh_build", "nexd_mesh_desc", "nexd_mesh_get_info", "nexd_mesh_write_seismograms",
                 "nexd_mesh_last_error", "nexd_mesh_free"]
 GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
-               "nexd_get_state", "nexd_set_state", "nexd_step_io", "nexd_profile_enable", "nexd_profile_get",
+               "nexd_get_state", "nexd_set_state", "nexd_step_io", "nexd_pml_trigger", "nexd_get_energy",
+               "nexd_profile_enable", "nexd_profile_get",
                "nexd_last_error", "nexd_launch_count", "nexd_destroy"]
-NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_COUNT = 0, 1, 2, 3
+NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_ENERGY, NEXD_K_COUNT = 0, 1, 2, 3, 4
 
 
 class NexdProfile(C.Structure):
@@ -117,6 +118,8 @@ def gpu_lib():
         lib.nexd_get_state.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_float)]
         lib.nexd_set_state.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_float)]
         lib.nexd_step_io.argtypes = [vp, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        lib.nexd_pml_trigger.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_int32]
+        lib.nexd_get_energy.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.nexd_profile_enable.argtypes = [vp, C.c_int32]
         lib.nexd_profile_get.argtypes = [vp, C.POINTER(NexdProfile)]
         lib.nexd_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]

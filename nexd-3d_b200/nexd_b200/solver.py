@@ -82,10 +82,26 @@ class Solver:
             return None
         p = _abi.NexdProfile()
         lib.nexd_profile_get(self._ctx, C.byref(p))
-        names = ("record", "stage_pml", "stage_main")
+        names = ("record", "stage_pml", "stage_main", "energy")
         out = {n: dict(launches=p.launches[i], ms=p.ms[i], elements=p.elements[i]) for i, n in enumerate(names)}
         out["span_ms"] = p.span_ms
         return out
+
+    def pml_trigger(self, avg_window1=10, avg_window2=2, sta_lta_trigger=0.1, f0=1.0, formula=0):
+        """Arm the NPML energy STA/LTA trigger (src/timeloopMod.f90:508-542)."""
+        st = _abi.gpu_lib().nexd_pml_trigger(self._ctx, avg_window1, avg_window2, sta_lta_trigger, f0, formula)
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+
+    def energy(self):
+        """(energy history (nt, nbatch), step at which the NPML switched off per wavefield)."""
+        e = np.zeros((self.nt, self.nbatch), dtype=np.float64, order="F")
+        sw = np.zeros(self.nbatch, dtype=np.int32)
+        st = _abi.gpu_lib().nexd_get_energy(self._ctx, e.ctypes.data_as(C.POINTER(C.c_double)),
+                                            sw.ctypes.data_as(C.POINTER(C.c_int32)))
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+        return e, sw
 
     def launch_count(self):
         n = C.c_int64()

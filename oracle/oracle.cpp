@@ -105,6 +105,89 @@ struct Oracle {
 
   // state of one batch member
   std::vector<R> q, qm, qn, rq, th, thm, thn, arq, aux, auxm, auxn, auxr, resq, resth, resaux, ux, ax;
+  // NPML trigger (src/timeloopMod.f90:508-542)
+  bool trig = false;
+  int tw1 = 10, tw2 = 2, tformula = 0, timecrit = 0;
+  double tthr = 0.1;
+  std::vector<double> mass;  // (Np,Np) column-major, M = (V V^T)^-1
+  double* energy_out = nullptr;
+  int* switch_out = nullptr;
+
+  void arm(int w1, int w2, double thr, double f0, int formula) {
+    trig = true;
+    tw1 = w1;
+    tw2 = w2;
+    tthr = thr;
+    tformula = formula;
+    timecrit = int(float(2.4 / f0 / d.dt));
+    // mass = inverse of invmass (Gauss-Jordan, partial pivoting)
+    std::vector<double> A(d.invmass, d.invmass + size_t(Np) * Np);
+    mass.assign(size_t(Np) * Np, 0.0);
+    for (int i = 0; i < Np; ++i) mass[size_t(i) * Np + i] = 1.0;
+    for (int c = 0; c < Np; ++c) {
+      int p = c;
+      for (int r = c + 1; r < Np; ++r)
+        if (std::fabs(A[size_t(c) * Np + r]) > std::fabs(A[size_t(c) * Np + p])) p = r;
+      for (int j = 0; j < Np; ++j) {
+        std::swap(A[size_t(j) * Np + c], A[size_t(j) * Np + p]);
+        std::swap(mass[size_t(j) * Np + c], mass[size_t(j) * Np + p]);
+      }
+      const double piv = A[size_t(c) * Np + c];
+      for (int j = 0; j < Np; ++j) { A[size_t(j) * Np + c] /= piv; mass[size_t(j) * Np + c] /= piv; }
+      for (int r = 0; r < Np; ++r) {
+        if (r == c) continue;
+        const double f = A[size_t(c) * Np + r];
+        for (int j = 0; j < Np; ++j) {
+          A[size_t(j) * Np + r] -= f * A[size_t(j) * Np + c];
+          mass[size_t(j) * Np + r] -= f * mass[size_t(j) * Np + c];
+        }
+      }
+    }
+  }
+
+  // energy_loc(it) of src/timeloopMod.f90:491-514 for the current q
+  double energy() const {
+    double total = 0.0;
+#pragma omp parallel for reduction(+ : total) schedule(static)
+    for (int e = 0; e < K; ++e) {
+      const size_t g0 = size_t(e) * Np;
+      const double lam = d.lambdau[e], mu = d.muu[e], rho = d.rho[e];
+      std::vector<double> x(size_t(15) * Np);  // v (3), e (6), q1..q6
+      for (int j = 0; j < Np; ++j) {
+        double qq[9];
+        for (int c = 0; c < 9; ++c) qq[c] = double(q[size_t(c) * ng + g0 + j]);
+        double ev[6];
+        if (tformula == 0) {
+          const double t1 = 1.0 / (4 * mu * mu + 6 * mu * lam);
+          ev[0] = (2 * (lam + mu) * qq[0] - lam * (qq[1] + qq[2])) / t1;
+          ev[1] = (2 * (lam + mu) * qq[1] - lam * (qq[0] + qq[2])) / t1;
+          ev[2] = (2 * (lam + mu) * qq[2] - lam * (qq[0] + qq[0])) / t1;
+        } else {
+          const double t1 = 4 * mu * mu + 6 * mu * lam;
+          ev[0] = (2 * (lam + mu) * qq[0] - lam * (qq[1] + qq[2])) / t1;
+          ev[1] = (2 * (lam + mu) * qq[1] - lam * (qq[0] + qq[2])) / t1;
+          ev[2] = (2 * (lam + mu) * qq[2] - lam * (qq[0] + qq[1])) / t1;
+        }
+        for (int c = 3; c < 6; ++c) ev[c] = qq[c] / (2 * mu);
+        for (int c = 0; c < 3; ++c) x[size_t(c) * Np + j] = qq[6 + c];
+        for (int c = 0; c < 6; ++c) x[size_t(3 + c) * Np + j] = ev[c];
+        for (int c = 0; c < 6; ++c) x[size_t(9 + c) * Np + j] = qq[c];
+      }
+      auto quad = [&](int a, int b) {  // x_a^T M x_b
+        double s = 0.0;
+        for (int n = 0; n < Np; ++n) {
+          double mb = 0.0;
+          for (int k = 0; k < Np; ++k) mb += mass[size_t(k) * Np + n] * x[size_t(b) * Np + k];
+          s += x[size_t(a) * Np + n] * mb;
+        }
+        return s;
+      };
+      const double kin = rho * (quad(0, 0) + quad(1, 1) + quad(2, 2));
+      const double pot = quad(9, 3) + quad(10, 4) + quad(11, 5) + 2 * (quad(12, 6) + quad(13, 7) + quad(14, 8));
+      total += 0.5 * d.jacobian[e] * (kin + pot);
+    }
+    return total;
+  }
 
   explicit Oracle(const nexd_desc& desc) : d(desc) {
     K = d.nelem;
@@ -565,6 +648,22 @@ struct Oracle {
             }
         }
       }
+      if (trig && pml) {
+        double* E = energy_out + size_t(batch) * nt;
+        E[it - 1] = energy();
+        if (switch_out[batch] == 0 && it > timecrit) {
+          float avg1 = 0.f, avg2 = 0.f;
+          for (int i = 1; i <= tw1; ++i)
+            if (it - i > 0) avg1 += float(E[it - i - 1] / tw1);
+          for (int i = 1; i <= tw2; ++i)
+            if (it - i > 0) avg2 += float(E[it - i - 1] / tw2);
+          const float sta_lta = avg2 / avg1;
+          if (std::fabs(sta_lta - 1.f) > float(tthr)) {
+            switch_out[batch] = it;  // pmlcheck(:) = .false.
+            std::fill(pmlc.begin(), pmlc.end(), 0);
+          }
+        }
+      }
       bool finite = true;
       for (size_t g = 0; g < ng && finite; g += 97) finite = std::isfinite(double(q[size_t(6) * ng + g]));
       if (!finite) throw std::runtime_error("non-finite wavefield in the oracle");
@@ -574,11 +673,29 @@ struct Oracle {
   }
 };
 
+struct TriggerCfg {
+  int w1, w2, formula;
+  double thr, f0;
+  double* energy;
+  int* sw;
+};
+
 template <class R>
-int run_t(const nexd_desc* d, int it_end, float* traces, double* field) {
+int run_t(const nexd_desc* d, int it_end, float* traces, double* field, const TriggerCfg* tc = nullptr) {
   Oracle<R> o(*d);
   std::fill(traces, traces + size_t(d->nrec) * d->nt * 9 * std::max(1, d->nbatch), 0.0f);
-  for (int b = 0; b < std::max(1, d->nbatch); ++b) o.run(it_end, traces, field, b);
+  const int nb = std::max(1, d->nbatch);
+  if (tc) {
+    o.arm(tc->w1, tc->w2, tc->thr, tc->f0, tc->formula);
+    o.energy_out = tc->energy;
+    o.switch_out = tc->sw;
+    std::fill(tc->energy, tc->energy + size_t(nb) * d->nt, 0.0);
+    std::fill(tc->sw, tc->sw + nb, 0);
+  }
+  for (int b = 0; b < nb; ++b) {
+    if (o.pml) o.pmlc.assign(d->pmlcheck, d->pmlcheck + d->nelem);
+    o.run(it_end, traces, field, b);
+  }
   return 0;
 }
 
@@ -623,6 +740,24 @@ int oracle_run(const nexd_desc* d, int precision, int it_end, float* traces, dou
 #endif
   try {
     return precision == 32 ? run_t<float>(d, it_end, traces, field) : run_t<double>(d, it_end, traces, field);
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return NEXD_ERR_NONFINITE;
+  }
+}
+
+int oracle_run_trigger(const nexd_desc* d, int precision, int it_end, float* traces, double* field, int nthreads,
+                       int avg_window1, int avg_window2, double sta_lta_trigger, double f0, int formula,
+                       double* energy, int* pml_switch) {
+  if (!check_desc(d) || !traces || !energy || !pml_switch) return NEXD_ERR_INVALID;
+  if (!d->set_pml) { g_err = "the trigger needs set_pml"; return NEXD_ERR_INVALID; }
+  if (it_end < 0 || it_end > d->nt) { g_err = "it_end out of range"; return NEXD_ERR_INVALID; }
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  TriggerCfg tc{avg_window1, avg_window2, formula, sta_lta_trigger, f0, energy, pml_switch};
+  try {
+    return precision == 32 ? run_t<float>(d, it_end, traces, field, &tc) : run_t<double>(d, it_end, traces, field, &tc);
   } catch (const std::exception& e) {
     g_err = e.what();
     return NEXD_ERR_NONFINITE;

@@ -35,6 +35,14 @@ int oracle_run(const nexd_desc* d, int precision, int it_end, float* traces, dou
 int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const double* q, const double* theta,
                const double* aux, double* rq, double* arq, double* auxr);
 
+/* oracle_run with the reference's NPML energy and STA/LTA trigger
+ * (src/timeloopMod.f90:482-542) armed: energy (nt, nbatch) FP64 history,
+ * pml_switch (nbatch) step at which the NPML was switched off (0 = never).
+ * formula 0: the reference's strain expression; 1: isotropic compliance. */
+int oracle_run_trigger(const nexd_desc* d, int precision, int it_end, float* traces, double* field, int nthreads,
+                       int avg_window1, int avg_window2, double sta_lta_trigger, double f0, int formula,
+                       double* energy, int* pml_switch);
+
 int oracle_last_error(char* buf, size_t len);
 
 #ifdef __cplusplus

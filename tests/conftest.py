@@ -48,7 +48,23 @@ def oracle(built):
     lib.oracle_run.restype = C.c_int
     lib.oracle_rhs.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 6
     lib.oracle_rhs.restype = C.c_int
+    lib.oracle_run_trigger.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_void_p,
+                                       C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    lib.oracle_run_trigger.restype = C.c_int
     return lib
+
+
+def run_oracle_trigger(lib, mesh, precision=64, w1=10, w2=2, thr=0.1, f0=1.0, formula=0):
+    """Oracle run with the NPML energy trigger armed: (traces, energy, switch)."""
+    tr = np.zeros((mesh.nrec, mesh.nt, 9, mesh.nbatch), dtype=np.float32, order="F")
+    en = np.zeros((mesh.nt, mesh.nbatch), dtype=np.float64, order="F")
+    sw = np.zeros(mesh.nbatch, dtype=np.int32)
+    st = lib.oracle_run_trigger(mesh.desc_ptr, precision, mesh.nt, tr.ctypes.data_as(C.POINTER(C.c_float)), None, 0,
+                                w1, w2, thr, f0, formula, en.ctypes.data_as(C.POINTER(C.c_double)),
+                                sw.ctypes.data_as(C.POINTER(C.c_int)))
+    assert st == 0, f"oracle failed with status {st}"
+    return tr, en, sw
 
 
 def run_oracle(lib, mesh, precision=64, steps=None, want_field=False):

@@ -12,7 +12,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import (brick_dt_cfl, pin_brick_edge_stations, rel_l2, run_oracle, trace_misfit, station_misfit, write_brick)
+from conftest import (brick_dt_cfl, pin_brick_edge_stations, rel_l2, run_oracle, run_oracle_trigger, trace_misfit,
+                      station_misfit, write_brick)
 from nexd_b200 import Mesh, NexdError, synth
 from nexd_b200 import _abi
 
@@ -179,3 +180,25 @@ def test_step_range_and_nonfinite_errors(tmp_path, Solver):
     with pytest.raises(NexdError) as ei:
         s.run(1, 2)
     assert ei.value.status == _abi.NEXD_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("formula", [0, 1])
+def test_pml_energy_trigger_matches_oracle(tmp_path, oracle, Solver, formula):
+    """Device energy reduction and STA/LTA trigger vs the oracle: energy history
+    within 1e-5, the same switch-off step, and matching traces afterwards."""
+    d = str(tmp_path / "pml")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=80, nrec=4, src_depth=(800.0, 800.0))
+    m = Mesh(d, N=3, stf_stage_time=True)
+    f0 = 10.0  # trigger frequency parameter: timecrit = 2.4/(f0 dt) = 34 steps here
+    for thr in (1e30, 1e-3):
+        s = Solver(m.desc_ptr)
+        s.pml_trigger(10, 2, thr, f0, formula)
+        s.run(1, 80)
+        eg, swg = s.energy()
+        tg = s.traces()
+        to, eo, swo = run_oracle_trigger(oracle, m, 64, thr=thr, f0=f0, formula=formula)
+        assert rel_l2(eg, eo) < 1e-5
+        assert swg[0] == swo[0]
+        assert trace_misfit(tg[..., 0], to[..., 0]) < 1e-4
+        if thr < 1 and formula == 1:
+            assert swg[0] > 0

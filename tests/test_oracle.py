@@ -5,7 +5,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import (brick_dt_cfl, pin_brick_edge_stations, run_oracle, trace_misfit, station_misfit, write_brick, rel_l2)
+from conftest import (brick_dt_cfl, pin_brick_edge_stations, run_oracle, run_oracle_trigger, trace_misfit,
+                      station_misfit, write_brick, rel_l2)
 from nexd_b200 import Mesh, synth
 
 
@@ -98,3 +99,32 @@ def test_batch_members_are_independent(tmp_path, oracle):
     ts = run_oracle(oracle, ms, 64)[..., 0]
     # the single run has both sources in one wavefield: linear superposition
     assert rel_l2(tb[..., 0] + tb[..., 1], ts) < 1e-5
+
+
+def _pml_model(tmp_path, nt=60):
+    d = str(tmp_path / "pml")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=nt, nrec=4, attenuation=False, src_depth=(800.0, 800.0))
+    return Mesh(d, N=2, stf_stage_time=True)
+
+
+def test_pml_energy_and_trigger(tmp_path, oracle):
+    """The reference's NPML STA/LTA safeguard (src/timeloopMod.f90:508-542):
+    the energy is non-negative with the physical compliance, a huge threshold
+    never fires (traces unchanged), a tiny one fires right after timecrit and
+    switches the NPML off."""
+    m = _pml_model(tmp_path)
+    base = run_oracle(oracle, m, 64)
+    f0 = 10.0  # trigger frequency parameter: timecrit = 2.4/(f0 dt) steps
+    timecrit = int(np.float32(2.4 / f0 / m.dt))
+    assert timecrit < m.nt - 5
+    tr, en, sw = run_oracle_trigger(oracle, m, 64, thr=1e30, f0=f0, formula=1)
+    assert sw[0] == 0 and (en[:, 0] >= 0).all() and en[-1, 0] > 0
+    assert rel_l2(tr, base) == 0.0
+    tr2, en2, sw2 = run_oracle_trigger(oracle, m, 64, thr=1e-9, f0=f0, formula=1)
+    assert sw2[0] == timecrit + 1
+    assert rel_l2(tr2, base) > 0.0
+    # The reference's own strain expression multiplies by 4mu^2+6mu*lambda
+    # (src/timeloopMod.f90:493-497); at these amplitudes the FP32 window
+    # averages overflow, the ratio is NaN and the trigger never fires.
+    tr3, en3, sw3 = run_oracle_trigger(oracle, m, 64, thr=1e-9, f0=f0, formula=0)
+    assert sw3[0] == 0 and np.isfinite(en3).all()
