@@ -189,6 +189,34 @@ int nexd_pml_trigger(nexd_ctx* ctx, int32_t avg_window1, int32_t avg_window2, do
  * (0 = never), the `pmlswitch` of the reference. */
 int nexd_get_energy(nexd_ctx* ctx, double* energy, int32_t* pml_switch);
 
+/* Wavefield energy of nbatch wavefields, computed from caller-provided device
+ * arrays without allocating any device memory.  This entry point has no
+ * counterpart in the reference: it exists for hosts that cannot call
+ * cudaMalloc while they monitor a run -- a host whose device memory is owned
+ * by another allocator (a framework's caching allocator or a pool reserved up
+ * front, as an MPI Fortran host may do), or monitoring code that must not
+ * incur cudaMalloc's implicit device synchronisation.
+ *
+ * Same computation as the trigger's energy (nexd_pml_trigger, formula 0 or 1);
+ * the block partial sums go to a fixed scratch array inside libnexd.so
+ * (NEXD_NOALLOC_MAX_BATCH wavefields x 256 blocks of FP64, 128 KiB), held by
+ * every GPU that loads the library until the process exits.
+ *   q:      device, field-major (nelem*Np nodes per field), field stride ldq,
+ *           wavefield stride 9*ldq
+ *   emat:   device, (4, nelem) FP32: rho, lambda, mu, J per element
+ *   mass:   device, (Np, Np) FP64 mass matrix
+ *   energy: host, nbatch FP64 results
+ * nbatch above NEXD_NOALLOC_MAX_BATCH is rejected with NEXD_ERR_INVALID.  The
+ * first call on a device looks up the scratch array's device address for that
+ * device (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Calls share the scratch array and leave their partial sums in it;
+ * calls that overlap on the GPU (other threads, other streams) race on it.
+ * Kernels run on the legacy default stream; the call returns after the
+ * results are copied to `energy`. */
+#define NEXD_NOALLOC_MAX_BATCH 64
+int nexd_wavefield_energy_noalloc(const float* q, int64_t ldq, int32_t nelem, int32_t Np, int32_t nbatch,
+                                  const float* emat, const double* mass, int32_t formula, double* energy);
+
 /* Kernel kinds reported by nexd_profile_get. */
 enum nexd_kernel_kind {
   NEXD_K_RECORD = 0,

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -91,6 +92,21 @@ struct nexd_ctx {
 };
 
 namespace {
+
+// Raises energy_kernel's dynamic shared-memory limit to the most the current
+// device allows for it (opt-in maximum minus its static shared memory).
+cudaError_t raise_energy_smem_limit() {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes fa{};
+  e = cudaFuncGetAttributes(&fa, nexd_dev::energy_kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(nexd_dev::energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              optin - int(fa.sharedSizeBytes));
+}
 
 int set_err(nexd_ctx* c, int code, const std::string& m) {
   if (c) c->err = m; else g_create_error = m;
@@ -807,9 +823,8 @@ int nexd_pml_trigger(nexd_ctx* c, int32_t avg_window1, int32_t avg_window2, doub
     if ((st = dalloc(c, &c->energy, size_t(c->nbatch) * c->nt)) ||
         (st = dalloc(c, &c->partials, size_t(c->nbatch) * c->energy_blocks)))
       return st;
-    const int E = kEnergyThreads / c->Np;
-    const size_t smem = (size_t(c->Np) * c->Np + size_t(E) * 9 * c->Np) * sizeof(double);
-    CUDA_TRY(c, cudaFuncSetAttribute(energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    // the attribute is an upper bound shared by all callers of energy_kernel
+    CUDA_TRY(c, raise_energy_smem_limit());
   }
   CUDA_TRY(c, cudaMemsetAsync(c->energy, 0, size_t(c->nbatch) * c->nt * sizeof(double), c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -830,6 +845,97 @@ int nexd_get_energy(nexd_ctx* c, double* energy, int32_t* pml_switch) {
   if (pml_switch)
     CUDA_TRY(c, cudaMemcpyAsync(pml_switch, c->pml_switch, c->nbatch * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return NEXD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Scratch of nexd_wavefield_energy_noalloc: FP64 block partials of up to
+// NEXD_NOALLOC_MAX_BATCH wavefields, then one total per wavefield.  Every GPU
+// that loads the library holds it until the process exits.
+constexpr int kNoAllocBlocks = 256;
+constexpr int kNoAllocSlots = NEXD_NOALLOC_MAX_BATCH * kNoAllocBlocks + NEXD_NOALLOC_MAX_BATCH;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlots];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current.  Host code must never pass the symbol itself to
+// a kernel: on the host it is only a stand-in, not a device address.
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[64] = {};
+
+// Fixed-order sum of each wavefield's partials into its total slot.
+__global__ void noalloc_sum(const double* partials, int nparts, double* totals) {
+  __shared__ double red[256];
+  const int b = blockIdx.x, tid = threadIdx.x;
+  double s = 0.0;
+  for (int i = tid; i < nparts; i += blockDim.x) s += partials[(long long)b * nparts + i];
+  red[tid] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (tid < w) red[tid] += red[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) totals[b] = red[0];
+}
+
+}  // namespace
+
+extern "C" {
+
+int nexd_wavefield_energy_noalloc(const float* q, int64_t ldq, int32_t nelem, int32_t Np, int32_t nbatch,
+                                  const float* emat, const double* mass, int32_t formula, double* energy) {
+  if (!q || !emat || !mass || !energy) return set_err(nullptr, NEXD_ERR_INVALID, "null argument");
+  if (nelem < 1 || Np < 1 || Np > kEnergyThreads || ldq < int64_t(nelem) * Np)
+    return set_err(nullptr, NEXD_ERR_INVALID, "bad sizes (need nelem >= 1, 1 <= Np <= 256, ldq >= nelem*Np)");
+  if (nbatch < 1 || nbatch > NEXD_NOALLOC_MAX_BATCH)
+    return set_err(nullptr, NEXD_ERR_INVALID, "nbatch must be 1..64 (size of the static scratch array)");
+  if (formula != 0 && formula != 1) return set_err(nullptr, NEXD_ERR_INVALID, "formula must be 0 or 1");
+  const int E = kEnergyThreads / Np;
+  const size_t smem = (size_t(Np) * Np + size_t(E) * 9 * Np) * sizeof(double);
+  if (smem > 200 * 1024) return set_err(nullptr, NEXD_ERR_UNSUPPORTED, "Np too large for the energy kernel");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return set_err(nullptr, NEXD_ERR_NODEVICE, "no usable CUDA device");
+  }
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      // one-time set-up on this device (this device is current)
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess)
+        return set_err(nullptr, NEXD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      e = raise_energy_smem_limit();
+      if (e != cudaSuccess)
+        return set_err(nullptr, NEXD_ERR_CUDA, std::string("energy kernel set-up: ") + cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  const int nchunk = (nelem + E - 1) / E;
+  const int nblk = std::max(1, std::min(kNoAllocBlocks, nchunk));
+  double* partials = scratch;                                   // [nbatch][nblk], every slot written
+  double* totals = scratch + NEXD_NOALLOC_MAX_BATCH * kNoAllocBlocks;  // [nbatch], every slot written
+  EnergyArgs ea{};
+  ea.K = nelem;
+  ea.Np = Np;
+  ea.nbatch = nbatch;
+  ea.ldq = ldq;
+  ea.q = q;
+  ea.emat = reinterpret_cast<const float4*>(emat);
+  ea.mass = mass;
+  ea.partials = partials;
+  ea.formula = formula;
+  energy_kernel<<<dim3(nblk, nbatch), kEnergyThreads, smem, 0>>>(ea);
+  noalloc_sum<<<nbatch, 256, 0, 0>>>(partials, nblk, totals);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(nullptr, NEXD_ERR_CUDA, std::string("energy launch: ") + cudaGetErrorString(e));
+  e = cudaMemcpy(energy, totals, size_t(nbatch) * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_err(nullptr, NEXD_ERR_CUDA, std::string("energy copy: ") + cudaGetErrorString(e));
   return NEXD_OK;
 }
 
