@@ -1,22 +1,33 @@
 """Throughput of the NEXD-3D time-stepping hot path on B200.
 
-Workload: the two-layer anelastic model with NPML (4 x 4 x 2 km, 40x40x20
-hexahedra x 6 = 192,000 tets, N=4, 3 Zener mechanisms, 3-cell NPML on the
-sides and bottom, free top, seeded double-couple source, 100 surface
+Default workload: the two-layer anelastic model with NPML (4 x 4 x 2 km,
+40x40x20 hexahedra x 6 = 192,000 tets, N=4, 3 Zener mechanisms, 3-cell NPML on
+the sides and bottom, free top, seeded double-couple source, 100 surface
 receivers, LSERK4), synthetic and seeded.  A step is one LSERK4 time step
 (5 stages) over the whole mesh.  Metric: DOF-stage updates per second,
-9 * Np * K * stages * steps / time (only the 9 velocity-stress fields count).
+9 * Np * K * stages * steps * wavefields / time (only the 9 velocity-stress
+fields count).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload twolayer|cube|batch64]
+
+Other workloads (measurements beside the headline, not the headline):
+  cube     homogeneous elastic 2 km cube, 6,000 tets, N=3, absorbing sides,
+           free top, vertical force, 9 receivers (the CPU-sized case)
+  batch64  the two-layer model with 64 independent moment-tensor sources in
+           one launch (64 wavefields, ~115 GB of state)
 
 value: device time (CUDA events on the library's stream) of K steps with the
-state resident in HBM (the ~4 GB of wavefield, residual, memory-variable and
-NPML arrays exceed the 126 MB L2 on every step).  e2e: K steps through the
-C-ABI streaming call nexd_step_io, each step copying its source samples in
-from the host and its receiver samples out, wall clock.  Under torchrun each
-rank runs an independent replica (its own seeded source); the time is the
-maximum over ranks.  --impl reference times the CPU restatement of the
-reference's solver (the oracle, FP32 like the reference) on the host cores.
+state resident in HBM, the steps replayed as captured CUDA graphs (the ~4 GB
+of wavefield, residual, memory-variable and NPML arrays exceed the 126 MB L2 on
+every step).  roofline: a second pass over K further steps with a CUDA event
+pair around every launch (steps launched one kernel at a time), which gives the
+per-kernel durations.  e2e: K steps through the C-ABI streaming call
+nexd_step_io, each step copying its source samples in from the host and its
+receiver samples out, wall clock.  Under torchrun each rank runs an independent
+replica (its own seeded source); the time is the maximum over ranks.
+--impl reference times the CPU restatement of the reference's solver (the
+oracle, FP32 like the reference) on the host cores.
 """
 import argparse
 import ctypes as C
@@ -37,10 +48,13 @@ sys.path.insert(0, PKG)
 
 from nexd_b200 import Mesh, synth, _abi  # noqa: E402
 
-WORKLOAD = "twolayer_anelastic_npml_192k_tets_N4_lserk4"
-CELLS = (40, 40, 20)
+WORKLOADS = {
+    "twolayer": dict(name="twolayer_anelastic_npml_192k_tets_N4_lserk4", cells=(40, 40, 20), N=4, nt=3000),
+    "cube": dict(name="cube_elastic_absorbing_6k_tets_N3_lserk4", cells=(10, 10, 10), N=3, nt=1000),
+    "batch64": dict(name="twolayer_anelastic_npml_192k_tets_N4_lserk4_64_sources", cells=(40, 40, 20), N=4,
+                    nt=2000, nsrc=64),
+}
 N_ORDER = 4
-NT = 3000
 # CPU sample: same model family and order at 20x20x10 cells (24,000 tets)
 CPU_SAMPLE_CELLS = (20, 20, 10)
 CPU_SAMPLE_STEPS = 6
@@ -133,13 +147,21 @@ def summarize_clocks(path, device):
             "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def oracle_baseline(tmp, steps=CPU_SAMPLE_STEPS):
+def oracle_baseline(tmp, workload="twolayer", steps=CPU_SAMPLE_STEPS):
     """FP32 CPU restatement of the reference solver on a bounded sample."""
     lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
     lib.oracle_run.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_void_p, C.c_int]
     d = os.path.join(tmp, "cpu_sample")
-    synth.write_twolayer(d, cells=CPU_SAMPLE_CELLS, nt=steps)
-    m = Mesh(d, N=N_ORDER, stf_stage_time=True)
+    if workload == "cube":
+        steps = 60
+        synth.write_cube(d, nt=steps)
+        m = Mesh(d, N=3, stf_stage_time=True)
+        what = f"{steps} LSERK4 steps of the full cube ({m.K} tets, N=3, elastic, absorbing)"
+    else:
+        synth.write_twolayer(d, cells=CPU_SAMPLE_CELLS, nt=steps)
+        m = Mesh(d, N=N_ORDER, stf_stage_time=True)
+        what = (f"{steps} LSERK4 steps of the same model family at {CPU_SAMPLE_CELLS[0]}x{CPU_SAMPLE_CELLS[1]}x"
+                f"{CPU_SAMPLE_CELLS[2]} cells ({m.K} tets, N={N_ORDER}, anelastic + NPML, one source)")
     tr = np.zeros((m.nrec, m.nt, 9, m.nbatch), dtype=np.float32, order="F")
     t0 = time.perf_counter()
     st = lib.oracle_run(m.desc_ptr, 32, steps, tr.ctypes.data_as(C.POINTER(C.c_float)), None, 0)
@@ -148,9 +170,7 @@ def oracle_baseline(tmp, steps=CPU_SAMPLE_STEPS):
         raise RuntimeError(f"oracle failed: {st}")
     units = 9 * m.Np * m.K * 5 * steps
     cores = os.cpu_count() or 1
-    sample = (f"{steps} LSERK4 steps of the same model family at {CPU_SAMPLE_CELLS[0]}x{CPU_SAMPLE_CELLS[1]}x"
-              f"{CPU_SAMPLE_CELLS[2]} cells ({m.K} tets, N={N_ORDER}, anelastic + NPML), FP32, "
-              f"{cores} OpenMP threads, {el:.1f} s")
+    sample = f"{what}, FP32, {cores} OpenMP threads, {el:.1f} s"
     return units / el, cores, sample
 
 
@@ -161,18 +181,21 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cells", default="40,40,20", help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
+    ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
+    ap.add_argument("--cells", default=None, help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
     args = ap.parse_args()
     rank, world, local, dist = dist_init()
-    cells = tuple(int(x) for x in args.cells.split(","))
-    workload = WORKLOAD if cells == CELLS else f"twolayer_anelastic_npml_{6 * cells[0] * cells[1] * cells[2]}_tets_N4_lserk4"
+    wl = WORKLOADS[args.workload]
+    cells = wl["cells"] if args.cells is None else tuple(int(x) for x in args.cells.split(","))
+    workload = wl["name"] if cells == wl["cells"] else \
+        wl["name"].replace("192k_tets", f"{6 * cells[0] * cells[1] * cells[2]}_tets")
     steps, warmup = args.steps, max(3, args.warmup)
     tmp = tempfile.mkdtemp(prefix=f"nexd_bench_{rank}_")
     metric = "DOF-stage updates/s"
     try:
         if args.impl == "reference":
             if rank == 0:
-                v, cores, sample = oracle_baseline(tmp)
+                v, cores, sample = oracle_baseline(tmp, args.workload)
                 line = {"metric": metric, "value": v, "unit": "DOF-stage/s", "n_gpus": args.gpus, "steps": steps,
                         "warmup": warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
                         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -187,32 +210,45 @@ def main():
         if dist is None:
             torch.cuda.set_device(0)
         d = os.path.join(tmp, "model")
-        synth.write_twolayer(d, cells=cells, nt=NT, nrec=100, src_seed=2 + rank)
-        mesh = Mesh(d, N=N_ORDER, stf_stage_time=True)
+        if args.workload == "cube":
+            synth.write_cube(d, cells=cells[0], nt=wl["nt"], seed=1 + rank)
+            mesh = Mesh(d, N=wl["N"], stf_stage_time=True)
+        else:
+            nsrc = wl.get("nsrc", 1)
+            kw = dict(src_depth=(500.0, 1800.0), f0_range=(2.0, 4.0)) if nsrc > 1 else {}
+            synth.write_twolayer(d, cells=cells, nt=wl["nt"], nrec=100, nsrc=nsrc, src_seed=2 + rank, **kw)
+            mesh = Mesh(d, N=wl["N"], stf_stage_time=True, nbatch=nsrc)
         s = Solver(mesh.desc_ptr)
         nstage = 5
-        need = warmup + 2 * steps
+        need = warmup + 3 * steps
         if need > mesh.nt:
-            raise SystemExit(f"--warmup + 2*--steps must be <= {mesh.nt}")
+            raise SystemExit(f"--warmup + 3*--steps must be <= {mesh.nt}")
         s.run(1, warmup)
         barrier(dist)
         torch.cuda.synchronize()
         clk_file = os.path.join(tmp, "clocks.csv")
         clk = sample_clocks(None, clk_file) if rank == 0 else None
         time.sleep(0.3 if clk else 0)
+        # timed region: K steps, CUDA graphs, run-span events only
         l0 = s.launch_count()
-        s.profile(True)
+        s.profile("span")
         barrier(dist)
+        torch.cuda.synchronize()
         s.run(warmup + 1, warmup + steps)
         torch.cuda.synchronize()
-        prof = s.profile()
+        span = s.profile()
         launches = s.launch_count() - l0
+        # roofline pass: K further steps, an event pair around every launch
+        s.profile(True)
+        s.run(warmup + steps + 1, warmup + 2 * steps)
+        torch.cuda.synchronize()
+        prof = s.profile()
         s.profile(False)
         if clk:
             clk.terminate()
             clk.wait()
-        dev_ms = max_over_ranks(dist, prof["span_ms"])
-        units = 9 * mesh.Np * mesh.K * nstage * steps
+        dev_ms = max_over_ranks(dist, span["span_ms"])
+        units = 9 * mesh.Np * mesh.K * nstage * steps * mesh.nbatch
         total_units = sum_over_ranks(dist, units)
         value = total_units / (dev_ms * 1e-3)
         # end to end through the streaming C-ABI call, host buffers in and out
@@ -223,7 +259,7 @@ def main():
         barrier(dist)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for it in range(warmup + steps + 1, warmup + 2 * steps + 1):
+        for it in range(warmup + 2 * steps + 1, warmup + 3 * steps + 1):
             stf_in[:, :] = stf_all[:, it - 1, :]
             s.step_io(it, stf_in, tr_out)
         e2e_s = max_over_ranks(dist, time.perf_counter() - t0)
@@ -232,9 +268,10 @@ def main():
             return
         peak, peak_kind = load_peaks()
         kinds = [k for k in ("stage_main", "stage_pml") if prof[k]["launches"] > 0]
+        nb = mesh.nbatch
         dom = max(kinds, key=lambda k: prof[k]["ms"])
         per_launch_ms = prof[dom]["ms"] / prof[dom]["launches"]
-        abytes = algorithmic_bytes(mesh, dom, prof[dom]["elements"])
+        abytes = algorithmic_bytes(mesh, dom, prof[dom]["elements"]) * nb
         achieved = abytes / (per_launch_ms * 1e-3) / 1e9
         traffic = None
         tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -246,17 +283,18 @@ def main():
                 traffic = None
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            v, cores, sample = oracle_baseline(tmp)
+            v, cores, sample = oracle_baseline(tmp, args.workload)
             cpu = {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
         clocks = summarize_clocks(clk_file, local) if clk else None
-        state_gb = (2 * 9 + 9 + 2 * 6 * mesh.desc.nMB) * mesh.K * mesh.Np * 4 / 1e9
+        state_gb = (2 * 9 + 9 + 2 * 6 * mesh.desc.nMB) * mesh.K * mesh.Np * 4 * nb / 1e9
         line = {
             "metric": metric, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded two-layer model, per-rank seeded source)",
             "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
                        "integrator": "LSERK4 (5 stages)", "pml_tets": int(prof["stage_pml"]["elements"]),
-                       "receivers": nrec, "sources_per_rank": nsrc,
+                       "receivers": nrec, "sources_per_rank": nsrc, "wavefields_per_rank": nb,
+                       "timed": "CUDA graphs of two steps; roofline from a per-launch-event pass of K more steps",
                        "l2": f"inputs larger than L2: {state_gb:.1f} GB of state streamed per stage",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -264,6 +302,7 @@ def main():
                          "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": per_launch_ms},
             "kernels": {k: {"launches": prof[k]["launches"], "ms": round(prof[k]["ms"], 3)}
                         for k in ("record", "stage_pml", "stage_main")},
+            "per_launch_pass_ms_per_step": prof["span_ms"] / steps,
             "e2e": {"value": e2e, "unit": "DOF-stage/s", "h2d_bytes_per_step": int(nspt * nsrc * 4),
                     "d2h_bytes_per_step": int(nrec * 9 * mesh.nbatch * 4)},
             "gpu_launches": int(launches),

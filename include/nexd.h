@@ -233,8 +233,10 @@ typedef struct nexd_profile {
   double span_ms;                 /* summed device time of whole nexd_run calls (first to last launch) */
 } nexd_profile;
 
-/* Enables (on != 0) or disables per-launch CUDA-event timing in nexd_run and
- * resets the counters. */
+/* Timing of nexd_run with CUDA events on the library's stream, counters reset:
+ * on = 0 off; 1 per-launch events per kernel kind plus the run span (steps are
+ * launched one kernel at a time); 2 run span only (steps replay captured
+ * two-step CUDA graphs, as without timing). */
 int nexd_profile_enable(nexd_ctx* ctx, int32_t on);
 int nexd_profile_get(const nexd_ctx* ctx, nexd_profile* out);
 

@@ -116,7 +116,8 @@ struct TriggerArgs {
   const double* partials;  // [nbatch][nparts]
   int nparts;
   double* energy;          // [nbatch][nt]
-  int nt, it;
+  int nt;
+  const int* it_dev;       // current step (1-based)
   int armed;               // STA/LTA active
   int timecrit;            // int(2.4 / f0 / dt)
   int w1, w2;
@@ -139,18 +140,19 @@ __global__ void energy_finalize(const TriggerArgs a) {
     __syncthreads();
   }
   if (tid != 0) return;
+  const int it = *a.it_dev;
   double* E = a.energy + (long long)b * a.nt;
-  E[a.it - 1] = red[0];
-  if (!a.armed || a.pml_off[b] || a.it <= a.timecrit) return;
+  E[it - 1] = red[0];
+  if (!a.armed || a.pml_off[b] || it <= a.timecrit) return;
   float avg1 = 0.f, avg2 = 0.f;
   for (int i = 1; i <= a.w1; ++i)
-    if (a.it - i > 0) avg1 += float(E[a.it - i - 1] / a.w1);
+    if (it - i > 0) avg1 += float(E[it - i - 1] / a.w1);
   for (int i = 1; i <= a.w2; ++i)
-    if (a.it - i > 0) avg2 += float(E[a.it - i - 1] / a.w2);
+    if (it - i > 0) avg2 += float(E[it - i - 1] / a.w2);
   const float sta_lta = avg2 / avg1;
   if (fabsf(sta_lta - 1.f) > a.threshold) {
     a.pml_off[b] = 1;
-    a.pml_switch[b] = a.it;
+    a.pml_switch[b] = it;
   }
 }
 

@@ -69,7 +69,8 @@ struct nexd_ctx {
   int64_t launches = 0;
   std::vector<void*> allocations;
   // profiling: CUDA events around each launch on `stream`
-  bool profiling = false;
+  bool profiling = false;  // per-launch events (mode 1)
+  bool span_timing = false; // run span events (modes 1 and 2)
   std::vector<cudaEvent_t> events;
   std::vector<int> ev_kind;  // kind of event pair i (events 2i, 2i+1)
   int ev_used = 0;
@@ -89,6 +90,12 @@ struct nexd_ctx {
   float4* emat = nullptr;      // [K] (rho, lambda, mu, J)
   double* mass = nullptr;      // [Np][Np]
   int energy_blocks = 0;
+  // step counter on the device and two-step CUDA graphs (one per starting buffer parity)
+  int* it_dev = nullptr;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int graph_launches = 0;      // kernels per captured two-step graph
+  bool graph_energy = false;   // energy_on when the graphs were captured
+  bool use_graphs = true;
 };
 
 namespace {
@@ -502,6 +509,8 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     if ((st = dalloc(c, &c->flag, 1))) return fail(st);
     CUDA_TRY(c, cudaMemset(c->flag, 0, sizeof(int)));
     if ((st = dalloc(c, &c->pml_off, size_t(nb))) || (st = dalloc(c, &c->pml_switch, size_t(nb)))) return fail(st);
+    if ((st = dalloc(c, &c->it_dev, 1))) return fail(st);
+    CUDA_TRY(c, cudaMemset(c->it_dev, 0, sizeof(int)));
     CUDA_TRY(c, cudaMemset(c->pml_off, 0, nb * sizeof(int)));
     CUDA_TRY(c, cudaMemset(c->pml_switch, 0, nb * sizeof(int)));
     // mass matrix M = (V V^T)^-1 and per-element energy constants, for the NPML trigger
@@ -595,8 +604,13 @@ void ev_collect(nexd_ctx* c) {
   c->ev_used = 0;
 }
 
-// Enqueues steps it_begin..it_end on the context's stream.
-void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
+__global__ void set_step_kernel(int* it_dev, int it) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *it_dev = it;
+}
+
+// Enqueues `nsteps` steps on the context's stream; the step number comes from
+// the device counter (set before, advanced by tick_kernel after each step).
+void enqueue_body(nexd_ctx* c, int nsteps) {
   const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
   size_t smem_p = 0, smem_m = 0;
   KernelFn kp = pick_kernel(c->N, c->att, true, mode, smem_p);
@@ -630,6 +644,7 @@ void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
   a.stf = c->stf;
   a.nt = c->nt;
   a.nspt = c->nspt;
+  a.it_dev = c->it_dev;
   a.rec_slot = c->rec_slot;
   a.abuf = c->abuf;
   a.nslot = std::max(1, c->nslot);
@@ -649,10 +664,10 @@ void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
   r.traces = c->traces;
   r.dt = float(c->dt);
   r.flag = c->flag;
+  r.it_dev = c->it_dev;
   const int rec_warps = c->nrec * c->nbatch;
-  for (int it = it_begin; it <= it_end; ++it) {
+  for (int step = 0; step < nsteps; ++step) {
     if (rec_warps > 0) {
-      r.it = it;
       r.q = c->qbuf[c->cur];
       const int threads = 128;
       const int blocks = (rec_warps * 32 + threads - 1) / threads;
@@ -661,7 +676,6 @@ void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
       ev_end(c, ev);
       ++c->launches;
     }
-    a.it = it;
     for (int s = 0; s < c->nstage; ++s) {
       a.stage = s;
       a.last_stage = (s == c->nstage - 1);
@@ -728,7 +742,7 @@ void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
       ta.nparts = c->energy_blocks;
       ta.energy = c->energy;
       ta.nt = c->nt;
-      ta.it = it;
+      ta.it_dev = c->it_dev;
       ta.armed = 1;
       ta.timecrit = c->trig_timecrit;
       ta.w1 = c->trig_w1;
@@ -740,7 +754,54 @@ void enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
       ev_end(c, ev);
       c->launches += 2;
     }
+    tick_kernel<<<1, 32, 0, c->stream>>>(c->it_dev);
+    ++c->launches;
   }
+}
+
+void drop_graphs(nexd_ctx* c) {
+  for (auto& g : c->gexec)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// Enqueues steps it_begin..it_end: pairs of steps replay a captured two-step
+// graph (the ping-pong parity returns to its start after two steps for every
+// integrator), a leftover single step and profiled runs launch directly.
+int enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
+  set_step_kernel<<<1, 32, 0, c->stream>>>(c->it_dev, it_begin);
+  int n = it_end - it_begin + 1;
+  if (c->profiling || !c->use_graphs || n < 2) {
+    enqueue_body(c, n);
+    return NEXD_OK;
+  }
+  if (c->graph_energy != c->energy_on) {
+    drop_graphs(c);
+    c->graph_energy = c->energy_on;
+  }
+  const int p = c->cur;
+  if (!c->gexec[p]) {
+    const int64_t before = c->launches;
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_body(c, 2);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->graph_launches = int(c->launches - before);  // kernels in the captured graph
+    c->launches = before;                           // counted when the graph runs
+    if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&c->gexec[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    if (c->cur != p) return set_err(c, NEXD_ERR_CUDA, "two-step graph changed the buffer parity");
+  }
+  for (; n >= 2; n -= 2) {
+    CUDA_TRY(c, cudaGraphLaunch(c->gexec[p], c->stream));
+    c->launches += c->graph_launches;
+  }
+  if (n == 1) enqueue_body(c, 1);
+  return NEXD_OK;
 }
 
 // Synchronises, collects profiling events and checks the non-finite flag.
@@ -760,17 +821,17 @@ int finish(nexd_ctx* c) {
 int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
   if (it_begin < 1 || it_end > c->nt || it_begin > it_end) return set_err(c, NEXD_ERR_INVALID, "step range out of 1..nt");
-  if (c->profiling) {
+  if (c->span_timing) {
     if (!c->span[0]) {
       CUDA_TRY(c, cudaEventCreate(&c->span[0]));
       CUDA_TRY(c, cudaEventCreate(&c->span[1]));
     }
     CUDA_TRY(c, cudaEventRecord(c->span[0], c->stream));
   }
-  enqueue_steps(c, it_begin, it_end);
-  if (c->profiling) CUDA_TRY(c, cudaEventRecord(c->span[1], c->stream));
+  if (int st = enqueue_steps(c, it_begin, it_end)) return st;
+  if (c->span_timing) CUDA_TRY(c, cudaEventRecord(c->span[1], c->stream));
   int st = finish(c);
-  if (c->profiling && st == NEXD_OK) {
+  if (c->span_timing && st == NEXD_OK) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, c->span[0], c->span[1]) == cudaSuccess) c->prof.span_ms += ms;
   }
@@ -792,7 +853,7 @@ int nexd_step_io(nexd_ctx* c, int32_t it, const float* stf_in, float* traces_out
                                   size_t(c->nspt) * sizeof(float), size_t(c->nspt) * sizeof(float), c->nsrc,
                                   cudaMemcpyHostToDevice, c->stream));
   }
-  enqueue_steps(c, it, it);
+  if (int st = enqueue_steps(c, it, it)) return st;
   if (nout > 0) {
     // (nrec, nt, 9*nbatch) column it-1 -> (nrec, 9*nbatch)
     CUDA_TRY(c, cudaMemcpy2DAsync(c->pinned + nin, size_t(c->nrec) * sizeof(float),
@@ -829,6 +890,7 @@ int nexd_pml_trigger(nexd_ctx* c, int32_t avg_window1, int32_t avg_window2, doub
   CUDA_TRY(c, cudaMemsetAsync(c->energy, 0, size_t(c->nbatch) * c->nt * sizeof(double), c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->energy_on = true;
+  drop_graphs(c);  // the captured trigger launches hold the old parameters
   return NEXD_OK;
 }
 
@@ -941,7 +1003,9 @@ int nexd_wavefield_energy_noalloc(const float* q, int64_t ldq, int32_t nelem, in
 
 int nexd_profile_enable(nexd_ctx* c, int32_t on) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
-  c->profiling = on != 0;
+  if (on < 0 || on > 2) return set_err(c, NEXD_ERR_INVALID, "timing mode must be 0, 1 or 2");
+  c->profiling = on == 1;
+  c->span_timing = on != 0;
   c->prof = nexd_profile{};
   c->prof.elements[NEXD_K_STAGE_PML] = c->Kpml;
   c->prof.elements[NEXD_K_STAGE_MAIN] = c->K - c->Kpml;
@@ -1050,6 +1114,7 @@ int nexd_launch_count(const nexd_ctx* c, int64_t* out) {
 int nexd_destroy(nexd_ctx* c) {
   if (!c) return NEXD_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
   for (void* p : c->allocations) cudaFree(p);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   for (cudaEvent_t e : c->span)

@@ -128,7 +128,8 @@ struct StageArgs {
   const int* src_batch;  // [nsrc]
   const float* src_pat;  // [nsrc][9][Np]
   const float* stf;      // [nsrc][nt][nspt]
-  int nt, nspt, it, stage;
+  int nt, nspt, stage;
+  const int* it_dev;     // current step (1-based), kept on the device so a captured step replays
   // receivers
   const int* rec_slot;   // [K] slot of receiver elements or -1
   float* abuf;           // [nbatch][nslot][3][Np]: last-stage rq(7:9)
@@ -691,7 +692,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     for (int s = a.src_head[e]; s >= 0; s = a.src_next[s]) {
       if (a.src_batch[s] != b) continue;
       const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
-      const float amp = a.stf[((long long)s * a.nt + (a.it - 1)) * a.nspt + sidx];
+      const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
       const float* p = a.src_pat + (long long)s * 9 * Np + n;
 #pragma unroll
       for (int c = 0; c < 9; ++c) rq[c] = fmaf(p[c * Np], amp, rq[c]);
@@ -730,7 +731,8 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
 
 // Receiver gather: one warp per (batch, receiver) (src/timeloopMod.f90:358-373).
 struct RecordArgs {
-  int nrec, nbatch, Np, nt, it;
+  int nrec, nbatch, Np, nt;
+  const int* it_dev;    // current step (1-based)
   long long ldq;
   const float* q;       // current wavefield
   const int* recelem;   // internal element of each receiver
@@ -769,21 +771,27 @@ __global__ void record_kernel(const RecordArgs a) {
       acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
     }
   if (lane == 0) {
+    const int it = *a.it_dev;
     float* u = a.u + ((long long)b * a.nrec + r) * 3;
     const long long tb = (long long)b * 9 * a.nt * a.nrec;
     bool bad = false;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       float uc = u[c];
-      if (a.it > 1) uc += a.dt * v[c];
+      if (it > 1) uc += a.dt * v[c];
       u[c] = uc;
-      a.traces[tb + ((long long)c * a.nt + (a.it - 1)) * a.nrec + r] = uc;
-      a.traces[tb + ((long long)(3 + c) * a.nt + (a.it - 1)) * a.nrec + r] = v[c];
-      a.traces[tb + ((long long)(6 + c) * a.nt + (a.it - 1)) * a.nrec + r] = acc[c];
+      a.traces[tb + ((long long)c * a.nt + (it - 1)) * a.nrec + r] = uc;
+      a.traces[tb + ((long long)(3 + c) * a.nt + (it - 1)) * a.nrec + r] = v[c];
+      a.traces[tb + ((long long)(6 + c) * a.nt + (it - 1)) * a.nrec + r] = acc[c];
       bad |= !isfinite(v[c]);
     }
     if (bad) atomicExch(a.flag, 1);
   }
+}
+
+// Advances the device step counter at the end of a step.
+__global__ void tick_kernel(int* it_dev) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *it_dev += 1;
 }
 
 }  // namespace nexd_dev

@@ -74,11 +74,13 @@ class Solver:
             raise _gpu_error(self._ctx, st)
 
     def profile(self, enable=None):
-        """Enable/disable CUDA-event timing (enable=True/False) or return the
-        per-kernel-kind counters as a dict."""
+        """CUDA-event timing: enable=True (per launch + run span), "span" (run
+        span only, CUDA graphs kept), False (off); without an argument return
+        the per-kernel-kind counters as a dict."""
         lib = _abi.gpu_lib()
         if enable is not None:
-            lib.nexd_profile_enable(self._ctx, 1 if enable else 0)
+            mode = 2 if enable == "span" else (1 if enable else 0)
+            lib.nexd_profile_enable(self._ctx, mode)
             return None
         p = _abi.NexdProfile()
         lib.nexd_profile_get(self._ctx, C.byref(p))
