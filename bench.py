@@ -181,6 +181,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--contraction", default="fp32", choices=["fp32", "bf16x3"],
+                    help="element contraction: FP32 CUDA cores or split-BF16 tcgen05 tensor cores")
     ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
     ap.add_argument("--cells", default=None, help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
     args = ap.parse_args()
@@ -219,6 +221,7 @@ def main():
             synth.write_twolayer(d, cells=cells, nt=wl["nt"], nrec=100, nsrc=nsrc, src_seed=2 + rank, **kw)
             mesh = Mesh(d, N=wl["N"], stf_stage_time=True, nbatch=nsrc)
         s = Solver(mesh.desc_ptr)
+        s.set_contraction(args.contraction)
         nstage = 5
         need = warmup + 3 * steps
         if need > mesh.nt:
@@ -292,7 +295,7 @@ def main():
             "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded two-layer model, per-rank seeded source)",
             "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
-                       "integrator": "LSERK4 (5 stages)", "pml_tets": int(prof["stage_pml"]["elements"]),
+                       "integrator": "LSERK4 (5 stages)", "contraction": args.contraction, "pml_tets": int(prof["stage_pml"]["elements"]),
                        "receivers": nrec, "sources_per_rank": nsrc, "wavefields_per_rank": nb,
                        "timed": "CUDA graphs of two steps; roofline from a per-launch-event pass of K more steps",
                        "l2": f"inputs larger than L2: {state_gb:.1f} GB of state streamed per stage",

@@ -233,6 +233,18 @@ typedef struct nexd_profile {
   double span_ms;                 /* summed device time of whole nexd_run calls (first to last launch) */
 } nexd_profile;
 
+/* Arithmetic of the per-element contraction (volume derivatives and LIFT):
+ * NEXD_CONTRACT_FP32 (default) FP32 on the CUDA cores, the reference's
+ * arithmetic (src/timeloopMod.f90:407-465 in FP32); NEXD_CONTRACT_BF16X3 the
+ * stacked [Dr Ds Dt LIFT] contraction on the tensor cores (tcgen05) with both
+ * operands split three ways into BF16 parts (h + m + l, 24 significant bits)
+ * and the six products above 2^-24 accumulated in FP32, order 4
+ * (NEXD_ERR_UNSUPPORTED otherwise).  The state, the stage update and
+ * everything else stay FP32.  No counterpart in the reference (its loop is
+ * FP32 matvecs). */
+enum nexd_contraction { NEXD_CONTRACT_FP32 = 0, NEXD_CONTRACT_BF16X3 = 1 };
+int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
+
 /* Timing of nexd_run with CUDA events on the library's stream, counters reset:
  * on = 0 off; 1 per-launch events per kernel kind plus the run span (steps are
  * launched one kernel at a time); 2 run span only (steps replay captured

@@ -17,6 +17,7 @@
 #include "../../include/nexd.h"
 #include "energy_kernel.cuh"
 #include "stage_kernel.cuh"
+#include "stage_tc.cuh"
 
 using namespace nexd_dev;
 
@@ -96,6 +97,9 @@ struct nexd_ctx {
   int graph_launches = 0;      // kernels per captured two-step graph
   bool graph_energy = false;   // energy_on when the graphs were captured
   bool use_graphs = true;
+  // element contraction: NEXD_CONTRACT_FP32 (CUDA cores) or NEXD_CONTRACT_BF16X3 (tensor cores)
+  int contraction = NEXD_CONTRACT_FP32;
+  uint4* ops_tc = nullptr;     // packed operator of the tensor-core kernels (orders 3 and 4)
 };
 
 namespace {
@@ -187,6 +191,73 @@ KernelFn pick_kernel(int N, bool att, bool pml, int mode, size_t& smem) {
   }
 }
 
+using TcKernelFn = void (*)(const StageArgs, const uint4*);
+
+template <int N>
+TcKernelFn pick_tc(bool att, bool pml, int mode) {
+  if (mode == MODE_LSERK) {
+    if (att) return pml ? stage_tc_kernel<N, true, true, MODE_LSERK> : stage_tc_kernel<N, true, false, MODE_LSERK>;
+    return pml ? stage_tc_kernel<N, false, true, MODE_LSERK> : stage_tc_kernel<N, false, false, MODE_LSERK>;
+  }
+  if (att) return pml ? stage_tc_kernel<N, true, true, MODE_TVD> : stage_tc_kernel<N, true, false, MODE_TVD>;
+  return pml ? stage_tc_kernel<N, false, true, MODE_TVD> : stage_tc_kernel<N, false, false, MODE_TVD>;
+}
+
+TcKernelFn pick_tc_kernel(int N, bool att, bool pml, int mode, size_t& smem) {
+  switch (N) {
+    case 4: smem = TcOrder<4>::smem_bytes(); return pick_tc<4>(att, pml, mode);
+    default: smem = 0; return nullptr;
+  }
+}
+
+// The stacked operator [Dr Ds Dt LIFT] of the tensor-core stage kernel as bf16
+// h, m, l rows (row n' = output node, K-major, 128-byte swizzle): entry
+// (n', d Np + k) = D_d(n', k), entry (n', KV16 + f NpF + i) = LIFT(n', f NpF + i),
+// zero elsewhere; x = h + m + l with m = bf16(x - h), l = bf16(x - h - m) of
+// the FP64 value.
+template <int N>
+std::vector<uint16_t> pack_tc_operator(const nexd_desc* d) {
+  using T = TcOrder<N>;
+  constexpr int Np = T::Np;
+  auto bf16_bits = [](double x) {
+    const float f = float(x);
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return uint16_t((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);  // round to nearest even
+  };
+  auto bf16_value = [](uint16_t h) {
+    const uint32_t u = uint32_t(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return double(f);
+  };
+  std::vector<uint16_t> out(T::B_BYTES / 2, 0);
+  for (int np_ = 0; np_ < Np; ++np_)
+    for (int k = 0; k < T::KU; ++k) {
+      double x = 0.0;
+      if (k < T::KV) {
+        const int dd = k / Np, kk = k - dd * Np;
+        const double* D = dd == 0 ? d->Dr : dd == 1 ? d->Ds : d->Dt;
+        x = D[size_t(kk) * Np + np_];
+      } else if (k >= T::KV16) {
+        x = d->lift[size_t(k - T::KV16) * Np + np_];
+      }
+      uint16_t part[3];
+      double r = x;
+      for (int q = 0; q < 3; ++q) {
+        part[q] = bf16_bits(r);
+        r -= bf16_value(part[q]);
+      }
+      for (int q = 0; q < 3; ++q) {
+        const int row = q * T::NP16 + np_, rr = row & 7, g = row >> 3, slab = k >> 6, kk = k & 63;
+        const size_t off = size_t(slab) * T::B_SLAB + size_t(g) * 1024 + size_t(rr) * 128 +
+                           size_t(((kk >> 3) ^ rr) << 4) + size_t(kk & 7) * 2;
+        out[off / 2] = part[q];
+      }
+    }
+  return out;
+}
+
 int elements_per_chunk(int N) {
   const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
   return 256 / Np;
@@ -247,6 +318,31 @@ int validate(const nexd_desc* d) {
 }  // namespace
 
 extern "C" {
+
+// Shared memory and persistent grid of the two stage kernels (NPML elements,
+// the rest) for the context's order, rheology, integrator and contraction.
+int configure_launch(nexd_ctx* c) {
+  const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
+  for (int which = 0; which < 2; ++which) {
+    const bool pmlk = which == 0;
+    size_t smem = 0;
+    const void* fn;
+    if (c->contraction == NEXD_CONTRACT_BF16X3) fn = reinterpret_cast<const void*>(pick_tc_kernel(c->N, c->att, pmlk, mode, smem));
+    else fn = reinterpret_cast<const void*>(pick_kernel(c->N, c->att, pmlk, mode, smem));
+    if (!fn) return set_err(c, NEXD_ERR_UNSUPPORTED, "no stage kernel for this order and contraction");
+    CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
+    if (per_sm < 1) return set_err(c, NEXD_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
+    const int nel = pmlk ? c->Kpml : c->K - c->Kpml;
+    const int E = elements_per_chunk(c->N);
+    const long long work = (long long)((nel + E - 1) / E) * c->nbatch;
+    const int grid = int(std::max<long long>(1, std::min<long long>(work, (long long)per_sm * c->nsm)));
+    if (pmlk) { c->grid_pml = grid; c->smem_pml = smem; }
+    else { c->grid_main = grid; c->smem_main = smem; }
+  }
+  return NEXD_OK;
+}
 
 int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   if (!out) return set_err(nullptr, NEXD_ERR_INVALID, "null output pointer");
@@ -550,23 +646,13 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     }
   }
   // ---- launch configuration ----
-  const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
-  for (int which = 0; which < 2; ++which) {
-    const bool pmlk = which == 0;
-    size_t smem = 0;
-    KernelFn fn = pick_kernel(N, c->att, pmlk, mode, smem);
-    if (!fn) return fail(set_err(c, NEXD_ERR_UNSUPPORTED, "no kernel for this order"));
-    CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    int per_sm = 0;
-    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
-    if (per_sm < 1) return fail(set_err(c, NEXD_ERR_UNSUPPORTED, "stage kernel does not fit on an SM"));
-    const int nel = pmlk ? c->Kpml : K - c->Kpml;
-    const int E = elements_per_chunk(N);
-    const long long work = (long long)((nel + E - 1) / E) * nb;
-    const int grid = int(std::max<long long>(1, std::min<long long>(work, (long long)per_sm * c->nsm)));
-    if (pmlk) { c->grid_pml = grid; c->smem_pml = smem; }
-    else { c->grid_main = grid; c->smem_main = smem; }
+  if (tc_order_supported(N)) {
+    std::vector<uint16_t> ops = pack_tc_operator<4>(d);
+    std::vector<uint4> ops4(ops.size() * 2 / sizeof(uint4));
+    std::memcpy(ops4.data(), ops.data(), ops4.size() * sizeof(uint4));
+    if ((st = upload(c, &c->ops_tc, ops4))) return fail(st);
   }
+  if ((st = configure_launch(c))) return fail(st);
   CUDA_TRY(c, cudaDeviceSynchronize());
   *out = c;
   return NEXD_OK;
@@ -613,9 +699,13 @@ __global__ void set_step_kernel(int* it_dev, int it) {
 void enqueue_body(nexd_ctx* c, int nsteps) {
   const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
   size_t smem_p = 0, smem_m = 0;
-  KernelFn kp = pick_kernel(c->N, c->att, true, mode, smem_p);
-  KernelFn km = pick_kernel(c->N, c->att, false, mode, smem_m);
+  const bool tcm = c->contraction == NEXD_CONTRACT_BF16X3;
+  KernelFn kp = tcm ? nullptr : pick_kernel(c->N, c->att, true, mode, smem_p);
+  KernelFn km = tcm ? nullptr : pick_kernel(c->N, c->att, false, mode, smem_m);
+  TcKernelFn tp = tcm ? pick_tc_kernel(c->N, c->att, true, mode, smem_p) : nullptr;
+  TcKernelFn tm = tcm ? pick_tc_kernel(c->N, c->att, false, mode, smem_m) : nullptr;
   StageArgs a{};
+  a.flag = c->flag;
   a.nbatch = c->nbatch;
   a.nMB = c->nMB;
   a.ldq = c->ldq;
@@ -707,7 +797,8 @@ void enqueue_body(nexd_ctx* c, int nsteps) {
         a.e_begin = 0;
         a.e_end = c->Kpml;
         const int ev = ev_begin(c, NEXD_K_STAGE_PML);
-        kp<<<c->grid_pml, 256, c->smem_pml, c->stream>>>(a);
+        if (tcm) tp<<<c->grid_pml, 256, c->smem_pml, c->stream>>>(a, c->ops_tc);
+        else kp<<<c->grid_pml, 256, c->smem_pml, c->stream>>>(a);
         ev_end(c, ev);
         ++c->launches;
       }
@@ -715,7 +806,8 @@ void enqueue_body(nexd_ctx* c, int nsteps) {
         a.e_begin = c->Kpml;
         a.e_end = c->K;
         const int ev = ev_begin(c, NEXD_K_STAGE_MAIN);
-        km<<<c->grid_main, 256, c->smem_main, c->stream>>>(a);
+        if (tcm) tm<<<c->grid_main, 256, c->smem_main, c->stream>>>(a, c->ops_tc);
+        else km<<<c->grid_main, 256, c->smem_main, c->stream>>>(a);
         ev_end(c, ev);
         ++c->launches;
       }
@@ -812,6 +904,7 @@ int finish(nexd_ctx* c) {
   CUDA_TRY(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (c->profiling) ev_collect(c);
+  if (flag & 2) return set_err(c, NEXD_ERR_CUDA, "tensor-core completion wait timed out in a stage kernel");
   if (flag) return set_err(c, NEXD_ERR_NONFINITE, "non-finite value in the wavefield at a receiver");
   return NEXD_OK;
 }
@@ -864,6 +957,24 @@ int nexd_step_io(nexd_ctx* c, int32_t it, const float* stf_in, float* traces_out
   int st = finish(c);
   if (st) return st;
   if (nout > 0) std::memcpy(traces_out, c->pinned + nin, nout * sizeof(float));
+  return NEXD_OK;
+}
+
+int nexd_set_contraction(nexd_ctx* c, int32_t mode) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (mode != NEXD_CONTRACT_FP32 && mode != NEXD_CONTRACT_BF16X3)
+    return set_err(c, NEXD_ERR_INVALID, "unknown contraction mode");
+  if (mode == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N))
+    return set_err(c, NEXD_ERR_UNSUPPORTED, "the tensor-core contraction covers order 4");
+  if (mode == c->contraction) return NEXD_OK;
+  const int old = c->contraction;
+  c->contraction = mode;
+  if (int st = configure_launch(c)) {
+    c->contraction = old;
+    configure_launch(c);
+    return st;
+  }
+  drop_graphs(c);
   return NEXD_OK;
 }
 

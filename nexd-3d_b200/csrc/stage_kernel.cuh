@@ -136,6 +136,7 @@ struct StageArgs {
   int nslot;
   int last_stage;
   const int* pml_off;    // [nbatch] 1 once the STA/LTA trigger switched the NPML off
+  int* flag;             // error bits: 1 non-finite trace (record kernel), 2 tensor-core wait timed out
 };
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
@@ -232,21 +233,15 @@ __device__ __forceinline__ Chunk chunk_of(const StageArgs& a, int w, int nchunk)
   return c;
 }
 
-// Issues the asynchronous copies of one chunk into a prefetch buffer:
-// element records (16-byte copies), own wavefield (field-major), the
-// neighbour face traces of interior faces (gathered through the face
-// patterns, using the connectivity `ids` staged one chunk earlier) and the
-// connectivity of the chunk after it (`next`, -1 for none).
+// Asynchronous copies of one chunk's element records (16-byte copies), own
+// wavefield (field-major), the connectivity of the chunk after it (`next`,
+// -1 for none) and the chunk's own face codes.  No commit.
 template <int N>
-__device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
-                                            const Chunk* next, const unsigned char* pat) {
+__device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, float* bGeo, float* bQ, int* bIds,
+                                           const Chunk* next) {
   using O = Order<N>;
-  constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E;
+  constexpr int Np = O::Np, E = O::E;
   const int tid = threadIdx.x, nth = blockDim.x;
-  float* bGeo = buf;
-  float* bQ = bGeo + O::SGEO;
-  float* bTr = bQ + O::SQF;
-  int* bIds = reinterpret_cast<int*>(bTr + O::STR);
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
   for (int i = tid; i < c.ne * 16; i += nth) cp_async16(bGeo + 4 * i, a.geo + (long long)c.e0 * GEO_STRIDE + 4 * i);
   const int cnt = c.ne * Np;
@@ -255,6 +250,25 @@ __device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, 
     const int f = i / (E * Np), r = i - f * (E * Np);
     if (r < cnt) cp_async4(bQ + i, qin + f * a.ldq + base + r);
   }
+  if (next)
+    for (int i = tid; i < next->ne * 2; i += nth) {
+      const int ee = i >> 1;
+      const int4* src = (i & 1) ? a.fcode + next->e0 + ee : a.nbr + next->e0 + ee;
+      cp_async16(bIds + ee * 12 + (i & 1) * 4, src);
+    }
+  for (int i = tid; i < c.ne; i += nth) cp_async16(bIds + i * 12 + 8, a.fcode + c.e0 + i);
+}
+
+// Asynchronous gather of the neighbour face traces of one chunk's interior
+// faces through the face patterns, using its connectivity `ids` (staged one
+// chunk earlier).  No commit.
+template <int N>
+__device__ __forceinline__ void issue_traces(const StageArgs& a, const Chunk& c, const int* ids, float* bTr,
+                                             const unsigned char* pat) {
+  using O = Order<N>;
+  constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
   for (int i = tid; i < c.ne * NF; i += nth) {
     const int ee = i / NF, j = i - ee * NF;
     const int f = j / NpF, fi = j - f * NpF;
@@ -267,19 +281,238 @@ __device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, 
       for (int k = 0; k < 9; ++k) cp_async4(dst + k, qin + k * a.ldq + gn);
     }
   }
-  if (next)
-    for (int i = tid; i < next->ne * 2; i += nth) {
-      const int ee = i >> 1;
-      const int4* src = (i & 1) ? a.fcode + next->e0 + ee : a.nbr + next->e0 + ee;
-      cp_async16(bIds + ee * 12 + (i & 1) * 4, src);
-    }
-  // this chunk's own face codes (the face phase reads them from here)
-  for (int i = tid; i < c.ne; i += nth) cp_async16(bIds + i * 12 + 8, a.fcode + c.e0 + i);
+}
+
+// All copies of one chunk into a prefetch buffer [records | wavefield |
+// traces | connectivity], committed as one group.
+template <int N>
+__device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
+                                            const Chunk* next, const unsigned char* pat) {
+  using O = Order<N>;
+  float* bGeo = buf;
+  float* bQ = bGeo + O::SGEO;
+  float* bTr = bQ + O::SQF;
+  int* bIds = reinterpret_cast<int*>(bTr + O::STR);
+  issue_main<N>(a, c, bGeo, bQ, bIds, next);
+  issue_traces<N>(a, c, ids, bTr, pat);
   cp_async_commit();
 }
 
 // Memory variables per mechanism set: the reference's nMB = 3 (src/constants.h:36).
 constexpr int kNMB = 3;
+
+// Update-phase state of one node, loaded into registers when the chunk starts
+// so the loads are in flight while the face, volume and lift terms run.  With
+// EARLY the per-element scalars of the tail (Zener coefficients, first
+// source, receiver slot, NPML switch) are prefetched too (kernels with one
+// block per SM, where their latency is not hidden); otherwise they are read
+// where they are used (kernels whose register budget is tight).
+template <bool ATT, bool PML, int MODE, bool EARLY = false>
+struct NodePrefetch {
+  static constexpr int NTH = ATT ? 6 * kNMB : 1;
+  static constexpr int NAX = PML ? 27 : 1;
+  float res[9], th[NTH], th2[NTH], ax[NAX], ax2[NAX], pr[PML ? 9 : 1];
+  float ae[(ATT && EARLY) ? 3 * kNMB : 1];  // per-element Zener coefficients
+  int src, slot, pml_off;                   // first source of the element, receiver slot, NPML switched off
+
+  __device__ __forceinline__ const float* zener(const StageArgs& a, int e) const {
+    return EARLY ? ae : a.ael + (long long)e * 3 * kNMB;
+  }
+  __device__ __forceinline__ int first_source(const StageArgs& a, int e) const { return EARLY ? src : a.src_head[e]; }
+  __device__ __forceinline__ int receiver_slot(const StageArgs& a, int e) const { return EARLY ? slot : a.rec_slot[e]; }
+  __device__ __forceinline__ bool npml_off(const StageArgs& a, int b) const { return EARLY ? pml_off != 0 : a.pml_off[b] != 0; }
+
+  template <int Np>
+  __device__ __forceinline__ void load(const StageArgs& a, int b, int e, long long node) {
+    const bool need2 = (MODE == MODE_LSERK) || !a.stage_first;
+    if (EARLY) {
+      src = __ldg(a.src_head + e);
+      slot = a.last_stage ? __ldg(a.rec_slot + e) : -1;
+      pml_off = PML ? a.pml_off[b] : 0;
+      if (ATT) {
+#pragma unroll
+        for (int j = 0; j < 3 * kNMB; ++j) ae[j] = __ldg(a.ael + (long long)e * 3 * kNMB + j);
+      }
+    }
+    if (MODE == MODE_LSERK) {
+      const float* rs = a.res + (long long)b * 9 * a.ldq + node;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) res[c] = __ldcs(rs + c * a.ldq);
+    } else if (a.ca != 0.f) {
+      const float* qn = a.q_n + (long long)b * 9 * a.ldq + node;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) res[c] = __ldcs(qn + c * a.ldq);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) res[c] = 0.f;
+    }
+    if (ATT) {
+      const float* t = a.th + (long long)b * 6 * kNMB * a.ldt + node;
+      const float* t2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
+#pragma unroll
+      for (int j = 0; j < NTH; ++j) th[j] = __ldcs(t + j * a.ldt);
+#pragma unroll
+      for (int j = 0; j < NTH; ++j) th2[j] = need2 ? __ldcs(t2 + j * a.ldt) : 0.f;
+    }
+    if (PML) {
+      const long long pn = node;  // PML elements come first internally, so node index = PML node index
+      const float* x = a.aux + (long long)b * 27 * a.lda + pn;
+      const float* x2 = a.aux2 + (long long)b * 27 * a.lda + pn;
+      const float* p = a.prof + (long long)e * 9 * Np + (node - (long long)e * Np);
+#pragma unroll
+      for (int i = 0; i < 27; ++i) ax[i] = __ldcs(x + i * a.lda);
+#pragma unroll
+      for (int i = 0; i < 27; ++i) ax2[i] = need2 ? __ldcs(x2 + i * a.lda) : 0.f;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) pr[i] = __ldg(p + i * Np);
+    }
+  }
+};
+
+// NPML auxiliary update of one node (src/timeloopMod.f90:399-405,
+// src/rungekuttaMod.f90:52-63) and the fluxes the volume term differentiates:
+// X, Y, Z = (F'+F)/kx, (G'+G)/ky, (H'+H)/kz, or F, G, H once the trigger
+// switched the layer off.  F, G, H are overwritten.
+template <bool ATT, int MODE, bool EARLY>
+__device__ __forceinline__ void pml_node(const StageArgs& a, int b, long long pn,
+                                         const NodePrefetch<ATT, true, MODE, EARLY>& p, float* F, float* G, float* H) {
+  if (p.npml_off(a, b)) return;  // pmlcheck(:) = .false.: ordinary element (src/timeloopMod.f90:537)
+  const float ddx = p.pr[0], ddy = p.pr[1], ddz = p.pr[2];
+  const float alx = p.pr[3], aly = p.pr[4], alz = p.pr[5];
+  const float ikx = 1.f / p.pr[6], iky = 1.f / p.pr[7], ikz = 1.f / p.pr[8];
+  float* aux = a.aux + (long long)b * 27 * a.lda + pn;
+  float* aux2 = a.aux2 + (long long)b * 27 * a.lda + pn;
+  const float* av = p.ax;
+  const float* a2 = p.ax2;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const float fp = av[i], gp = av[9 + i], hp = av[18 + i];
+    const float rf = -alx * fp - ddx * ikx * (fp + F[i]);
+    const float rg = -aly * gp - ddy * iky * (gp + G[i]);
+    const float rh = -alz * hp - ddz * ikz * (hp + H[i]);
+    const float phi = (fp + F[i]) * ikx, psi = (gp + G[i]) * iky, ome = (hp + H[i]) * ikz;
+    float nf, ng_, nh;
+    if (MODE == MODE_LSERK) {
+      const float r1 = a.ca * a2[i] + a.dt * rf;
+      const float r2 = a.ca * a2[9 + i] + a.dt * rg;
+      const float r3 = a.ca * a2[18 + i] + a.dt * rh;
+      __stcs(aux2 + i * a.lda, r1);
+      __stcs(aux2 + (9 + i) * a.lda, r2);
+      __stcs(aux2 + (18 + i) * a.lda, r3);
+      nf = fp + a.cb * r1;
+      ng_ = gp + a.cb * r2;
+      nh = hp + a.cb * r3;
+    } else {
+      float n1, n2, n3;
+      if (a.stage_first) {
+        __stcs(aux2 + i * a.lda, fp);
+        __stcs(aux2 + (9 + i) * a.lda, gp);
+        __stcs(aux2 + (18 + i) * a.lda, hp);
+        n1 = fp; n2 = gp; n3 = hp;
+      } else {
+        n1 = a2[i]; n2 = a2[9 + i]; n3 = a2[18 + i];
+      }
+      nf = a.ca * n1 + a.cb * (fp + a.dt * rf);
+      ng_ = a.ca * n2 + a.cb * (gp + a.dt * rg);
+      nh = a.ca * n3 + a.cb * (hp + a.dt * rh);
+    }
+    __stcs(aux + i * a.lda, nf);
+    __stcs(aux + (9 + i) * a.lda, ng_);
+    __stcs(aux + (18 + i) * a.lda, nh);
+    F[i] = phi;
+    G[i] = psi;
+    H[i] = ome;
+  }
+}
+
+// elasticFluxes (src/waveMod.f90:29-63) with e1..e4 = -(lambda+2mu), -lambda, -mu, -1/rho.
+__device__ __forceinline__ void elastic_fluxes(const float* g, const float* qv, float* F, float* G, float* H) {
+  const float e1 = g[G_E1], e2 = g[G_E2], e3 = g[G_E3], e4 = g[G_E4];
+  F[0] = e1 * qv[6]; F[1] = e2 * qv[6]; F[2] = e2 * qv[6]; F[3] = e3 * qv[7]; F[4] = 0.f;
+  F[5] = e3 * qv[8]; F[6] = e4 * qv[0]; F[7] = e4 * qv[3]; F[8] = e4 * qv[5];
+  G[0] = e2 * qv[7]; G[1] = e1 * qv[7]; G[2] = e2 * qv[7]; G[3] = e3 * qv[6]; G[4] = e3 * qv[8];
+  G[5] = 0.f; G[6] = e4 * qv[3]; G[7] = e4 * qv[1]; G[8] = e4 * qv[4];
+  H[0] = e2 * qv[8]; H[1] = e2 * qv[8]; H[2] = e1 * qv[8]; H[3] = 0.f; H[4] = e3 * qv[7];
+  H[5] = e3 * qv[6]; H[6] = e4 * qv[5]; H[7] = e4 * qv[4]; H[8] = e4 * qv[2];
+}
+
+// Everything after the spatial operator for one node: Zener memory variables
+// (src/timeloopMod.f90:426-461) driven by S = lifted anelastic flux - strain
+// rate, point sources (467-475), the receiver acceleration of the last stage,
+// and the stage update of q.  rq holds the volume + surface term on entry.
+template <int Np, bool ATT, bool PML, int MODE, bool EARLY>
+__device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, long long node, float* rq, const float* S,
+                                            const NodePrefetch<ATT, PML, MODE, EARLY>& p, const float* qown,
+                                            int qstride, const float* wls) {
+  const int n = int(node - (long long)e * Np);
+  if (ATT) {
+    float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
+    float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
+    const float* ae = p.zener(a, e);
+#pragma unroll
+    for (int l = 0; l < kNMB; ++l) {
+      const float wl = EARLY ? wls[l] : a.wl[l];
+      const float* t = p.th + 6 * l;
+      const float* t2 = p.th2 + 6 * l;
+      const float c1 = ae[3 * l], c2 = ae[3 * l + 1], c3 = ae[3 * l + 2];
+      rq[0] += c3 * t[0] + c1 * (t[1] + t[2]);
+      rq[1] += c3 * t[1] + c1 * (t[2] + t[0]);
+      rq[2] += c3 * t[2] + c1 * (t[0] + t[1]);
+      rq[3] += c2 * t[3];
+      rq[4] += c2 * t[4];
+      rq[5] += c2 * t[5];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const float r = wl * (S[j] - t[j]);
+        const long long o = (l * 6 + j) * a.ldt;
+        float nt_;
+        if (MODE == MODE_LSERK) {
+          const float rr = a.ca * t2[j] + a.dt * r;
+          __stcs(th2 + o, rr);
+          nt_ = t[j] + a.cb * rr;
+        } else {
+          float tn;
+          if (a.stage_first) { __stcs(th2 + o, t[j]); tn = t[j]; } else { tn = t2[j]; }
+          nt_ = a.ca * tn + a.cb * (t[j] + a.dt * r);
+        }
+        __stcs(th + o, nt_);
+      }
+    }
+  }
+  for (int s = p.first_source(a, e); s >= 0; s = a.src_next[s]) {
+    if (a.src_batch[s] != b) continue;
+    const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
+    const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
+    const float* sp = a.src_pat + (long long)s * 9 * Np + n;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) rq[c] = fmaf(sp[c * Np], amp, rq[c]);
+  }
+  if (a.last_stage) {
+    const int slot = p.receiver_slot(a, e);
+    if (slot >= 0) {
+      float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
+      ab[0] = rq[6];
+      ab[Np] = rq[7];
+      ab[2 * Np] = rq[8];
+    }
+  }
+  float* qo = a.q_out + (long long)b * 9 * a.ldq + node;
+  if (MODE == MODE_LSERK) {
+    float* rs = a.res + (long long)b * 9 * a.ldq + node;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const float r = a.ca * p.res[c] + a.dt * rq[c];
+      __stcs(rs + c * a.ldq, r);
+      __stcs(qo + c * a.ldq, qown[c * qstride] + a.cb * r);
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const float base = (a.ca != 0.f) ? a.ca * p.res[c] : 0.f;
+      __stcs(qo + c * a.ldq, base + a.cb * (qown[c * qstride] + a.dt * rq[c]));
+    }
+  }
+}
 
 template <int N, bool ATT, bool PML, int MODE>
 __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs a) {
@@ -303,6 +536,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       sAmp[(i >> 2) / 3 * O::AE + (i >> 2) % 3 * O::NFP + (i & 3) * 2 * O::NPAIR + NpF] = 0.f;
   for (int i = tid; i < a.npat * NpF; i += blockDim.x) sPat[i] = a.patterns[i];
 
+  const float* wls = nullptr;  // relaxation frequencies are read from a.wl where used
   const int nel = a.e_end - a.e_begin;
   const int nchunk = (nel + E - 1) / E;
   const int nwork = nchunk * a.nbatch;
@@ -343,44 +577,8 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     // terms are computed; one block per SM keeps them in registers)
     const bool active = le < ne;
     const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
-    constexpr int NTH = ATT ? 6 * kNMB : 1;
-    constexpr int NAX = PML ? 27 : 1;
-    float pre_res[9], pre_th[NTH], pre_th2[NTH], pre_ax[NAX], pre_ax2[NAX], pre_pr[PML ? 9 : 1];
-    const bool need2 = (MODE == MODE_LSERK) || !a.stage_first;
-    if (active) {
-      if (MODE == MODE_LSERK) {
-        const float* rs = a.res + (long long)b * 9 * a.ldq + node;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) pre_res[c] = __ldcs(rs + c * a.ldq);
-      } else if (a.ca != 0.f) {
-        const float* qn = a.q_n + (long long)b * 9 * a.ldq + node;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) pre_res[c] = __ldcs(qn + c * a.ldq);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) pre_res[c] = 0.f;
-      }
-      if (ATT) {
-        const float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
-        const float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
-#pragma unroll
-        for (int j = 0; j < NTH; ++j) pre_th[j] = __ldcs(th + j * a.ldt);
-#pragma unroll
-        for (int j = 0; j < NTH; ++j) pre_th2[j] = need2 ? __ldcs(th2 + j * a.ldt) : 0.f;
-      }
-      if (PML) {
-        const long long pn = (long long)(e0 + le) * Np + n;  // PML elements come first internally
-        const float* ax = a.aux + (long long)b * 27 * a.lda + pn;
-        const float* ax2 = a.aux2 + (long long)b * 27 * a.lda + pn;
-        const float* pr = a.prof + (long long)(e0 + le) * 9 * Np + n;
-#pragma unroll
-        for (int i = 0; i < 27; ++i) pre_ax[i] = __ldcs(ax + i * a.lda);
-#pragma unroll
-        for (int i = 0; i < 27; ++i) pre_ax2[i] = need2 ? __ldcs(ax2 + i * a.lda) : 0.f;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) pre_pr[i] = __ldg(pr + i * Np);
-      }
-    }
+    NodePrefetch<ATT, PML, MODE> pf;
+    if (active) pf.template load<Np>(a, b, e0 + le, node);
     // ---- start the next chunk's copies ------------------------------------------
     {
       const int wn = w + gridDim.x;
@@ -433,75 +631,20 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     // ---- PML: auxiliary update and contravariant modified fluxes ------------------
     float vgrad[9];  // d(v_c)/d(x_d) [c*3+d] (anelastic)
     (void)vgrad;
-    if (PML && active) {
-      const int e = e0 + le;
+    if constexpr (PML) if (active) {
       const float* g = sGeo + le * GEO_STRIDE;
       float qv[9];
 #pragma unroll
       for (int c = 0; c < 9; ++c) qv[c] = sQF[c * (E * Np) + le * Np + n];
       float F[9], G[9], H[9];
-      const float e1 = g[G_E1], e2 = g[G_E2], e3 = g[G_E3], e4 = g[G_E4];
-      F[0] = e1 * qv[6]; F[1] = e2 * qv[6]; F[2] = e2 * qv[6]; F[3] = e3 * qv[7]; F[4] = 0.f;
-      F[5] = e3 * qv[8]; F[6] = e4 * qv[0]; F[7] = e4 * qv[3]; F[8] = e4 * qv[5];
-      G[0] = e2 * qv[7]; G[1] = e1 * qv[7]; G[2] = e2 * qv[7]; G[3] = e3 * qv[6]; G[4] = e3 * qv[8];
-      G[5] = 0.f; G[6] = e4 * qv[3]; G[7] = e4 * qv[1]; G[8] = e4 * qv[4];
-      H[0] = e2 * qv[8]; H[1] = e2 * qv[8]; H[2] = e1 * qv[8]; H[3] = 0.f; H[4] = e3 * qv[7];
-      H[5] = e3 * qv[6]; H[6] = e4 * qv[5]; H[7] = e4 * qv[4]; H[8] = e4 * qv[2];
-      const long long pn = (long long)e * Np + n;  // PML elements come first in the internal order
-      const float ddx = pre_pr[0], ddy = pre_pr[1], ddz = pre_pr[2];
-      const float alx = pre_pr[3], aly = pre_pr[4], alz = pre_pr[5];
-      const float ikx = 1.f / pre_pr[6], iky = 1.f / pre_pr[7], ikz = 1.f / pre_pr[8];
-      float* aux = a.aux + (long long)b * 27 * a.lda + pn;
-      float* aux2 = a.aux2 + (long long)b * 27 * a.lda + pn;
+      elastic_fluxes(g, qv, F, G, H);
+      pml_node<ATT, MODE>(a, b, node, pf, F, G, H);
       float* cf = sCF + le * O::CFE + n * CS;
-      const float* av = pre_ax;
-      const float* a2 = pre_ax2;
-      if (a.pml_off[b]) {  // pmlcheck(:) = .false.: ordinary element (src/timeloopMod.f90:537)
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-          cf[i] = g[G_RX] * F[i] + g[G_RY] * G[i] + g[G_RZ] * H[i];
-          cf[10 + i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
-          cf[20 + i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
-        }
-      } else
 #pragma unroll
       for (int i = 0; i < 9; ++i) {
-        const float fp = av[i], gp = av[9 + i], hp = av[18 + i];
-        const float rf = -alx * fp - ddx * ikx * (fp + F[i]);
-        const float rg = -aly * gp - ddy * iky * (gp + G[i]);
-        const float rh = -alz * hp - ddz * ikz * (hp + H[i]);
-        const float phi = (fp + F[i]) * ikx, psi = (gp + G[i]) * iky, ome = (hp + H[i]) * ikz;
-        cf[i] = g[G_RX] * phi + g[G_RY] * psi + g[G_RZ] * ome;
-        cf[10 + i] = g[G_SX] * phi + g[G_SY] * psi + g[G_SZ] * ome;
-        cf[20 + i] = g[G_TX] * phi + g[G_TY] * psi + g[G_TZ] * ome;
-        float nf, ng_, nh;
-        if (MODE == MODE_LSERK) {
-          const float r1 = a.ca * a2[i] + a.dt * rf;
-          const float r2 = a.ca * a2[9 + i] + a.dt * rg;
-          const float r3 = a.ca * a2[18 + i] + a.dt * rh;
-          __stcs(aux2 + i * a.lda, r1);
-          __stcs(aux2 + (9 + i) * a.lda, r2);
-          __stcs(aux2 + (18 + i) * a.lda, r3);
-          nf = fp + a.cb * r1;
-          ng_ = gp + a.cb * r2;
-          nh = hp + a.cb * r3;
-        } else {
-          float n1, n2, n3;
-          if (a.stage_first) {
-            __stcs(aux2 + i * a.lda, fp);
-            __stcs(aux2 + (9 + i) * a.lda, gp);
-            __stcs(aux2 + (18 + i) * a.lda, hp);
-            n1 = fp; n2 = gp; n3 = hp;
-          } else {
-            n1 = a2[i]; n2 = a2[9 + i]; n3 = a2[18 + i];
-          }
-          nf = a.ca * n1 + a.cb * (fp + a.dt * rf);
-          ng_ = a.ca * n2 + a.cb * (gp + a.dt * rg);
-          nh = a.ca * n3 + a.cb * (hp + a.dt * rh);
-        }
-        __stcs(aux + i * a.lda, nf);
-        __stcs(aux + (9 + i) * a.lda, ng_);
-        __stcs(aux + (18 + i) * a.lda, nh);
+        cf[i] = g[G_RX] * F[i] + g[G_RY] * G[i] + g[G_RZ] * H[i];
+        cf[10 + i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
+        cf[20 + i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
       }
     }
     __syncthreads();
@@ -645,86 +788,18 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
         for (int c = 0; c < 6; ++c) sig_an[c] += NN[c] * A0 + X[c] * as;
       }
     }
-    // ---- Zener memory variables (src/timeloopMod.f90:426-461) ------------------
+    // ---- memory variables, sources, receivers, stage update ------------------------
+    float S[6];
     if (ATT) {
       // S = -strain rate + lifted anelastic flux; d theta_l/dt = w_l (S - theta_l)
-      float S[6];
       S[0] = sig_an[0] - vgrad[0];
       S[1] = sig_an[1] - vgrad[4];
       S[2] = sig_an[2] - vgrad[8];
       S[3] = sig_an[3] - 0.5f * (vgrad[3] + vgrad[1]);
       S[4] = sig_an[4] - 0.5f * (vgrad[7] + vgrad[5]);
       S[5] = sig_an[5] - 0.5f * (vgrad[6] + vgrad[2]);
-      float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
-      float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
-      const float* ae = a.ael + (long long)e * 3 * kNMB;
-#pragma unroll
-      for (int l = 0; l < kNMB; ++l) {
-        const float wl = a.wl[l];
-        const float* t = pre_th + 6 * l;
-        const float* t2 = pre_th2 + 6 * l;
-        const float c1 = ae[3 * l], c2 = ae[3 * l + 1], c3 = ae[3 * l + 2];
-        rq[0] += c3 * t[0] + c1 * (t[1] + t[2]);
-        rq[1] += c3 * t[1] + c1 * (t[2] + t[0]);
-        rq[2] += c3 * t[2] + c1 * (t[0] + t[1]);
-        rq[3] += c2 * t[3];
-        rq[4] += c2 * t[4];
-        rq[5] += c2 * t[5];
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-          const float r = wl * (S[j] - t[j]);
-          const long long o = (l * 6 + j) * a.ldt;
-          float nt_;
-          if (MODE == MODE_LSERK) {
-            const float rr = a.ca * t2[j] + a.dt * r;
-            __stcs(th2 + o, rr);
-            nt_ = t[j] + a.cb * rr;
-          } else {
-            float tn;
-            if (a.stage_first) { __stcs(th2 + o, t[j]); tn = t[j]; } else { tn = t2[j]; }
-            nt_ = a.ca * tn + a.cb * (t[j] + a.dt * r);
-          }
-          __stcs(th + o, nt_);
-        }
-      }
     }
-    // ---- point sources -----------------------------------------------------------
-    for (int s = a.src_head[e]; s >= 0; s = a.src_next[s]) {
-      if (a.src_batch[s] != b) continue;
-      const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
-      const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
-      const float* p = a.src_pat + (long long)s * 9 * Np + n;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) rq[c] = fmaf(p[c * Np], amp, rq[c]);
-    }
-    // ---- receiver acceleration (last stage) ----------------------------------------
-    if (a.last_stage) {
-      const int slot = a.rec_slot[e];
-      if (slot >= 0) {
-        float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
-        ab[0] = rq[6];
-        ab[Np] = rq[7];
-        ab[2 * Np] = rq[8];
-      }
-    }
-    // ---- stage update ------------------------------------------------------------
-    float* qo = a.q_out + (long long)b * 9 * a.ldq + node;
-    const float* qown = sQF + le * Np + n;
-    if (MODE == MODE_LSERK) {
-      float* rs = a.res + (long long)b * 9 * a.ldq + node;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) {
-        const float r = a.ca * pre_res[c] + a.dt * rq[c];
-        __stcs(rs + c * a.ldq, r);
-        __stcs(qo + c * a.ldq, qown[c * (E * Np)] + a.cb * r);
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 9; ++c) {
-        const float base = (a.ca != 0.f) ? a.ca * pre_res[c] : 0.f;
-        __stcs(qo + c * a.ldq, base + a.cb * (qown[c * (E * Np)] + a.dt * rq[c]));
-      }
-    }
+    finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, E * Np, wls);
   }
   cp_async_wait_all();
 }

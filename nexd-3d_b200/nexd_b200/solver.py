@@ -89,6 +89,14 @@ class Solver:
         out["span_ms"] = p.span_ms
         return out
 
+    def set_contraction(self, mode):
+        """Element contraction arithmetic: "fp32" (CUDA cores, default) or
+        "bf16x3" (tcgen05 tensor cores, split BF16, FP32 accumulation)."""
+        m = {"fp32": _abi.NEXD_CONTRACT_FP32, "bf16x3": _abi.NEXD_CONTRACT_BF16X3}.get(mode, mode)
+        st = _abi.gpu_lib().nexd_set_contraction(self._ctx, m)
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+
     def pml_trigger(self, avg_window1=10, avg_window2=2, sta_lta_trigger=0.1, f0=1.0, formula=0):
         """Arm the NPML energy STA/LTA trigger (src/timeloopMod.f90:508-542)."""
         st = _abi.gpu_lib().nexd_pml_trigger(self._ctx, avg_window1, avg_window2, sta_lta_trigger, f0, formula)

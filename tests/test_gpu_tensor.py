@@ -1,0 +1,152 @@
+"""The tensor-core contraction (NEXD_CONTRACT_BF16X3: tcgen05, both operands
+split three ways into BF16 parts, six products accumulated in FP32) against
+the FP64 oracle and against the FP32 CUDA-core path, through the C-ABI.
+
+Tolerances are those of the FP32 path: one right-hand side within 2e-5
+relative L2 of the oracle plus the FP32 loss of the Euler difference; receiver
+traces after the full run within 1e-4 relative L2 of the FP64 oracle, per
+trace kind.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2, run_oracle, trace_misfit
+from nexd_b200 import Mesh, NexdError, synth
+from nexd_b200 import _abi
+from test_gpu_parity import _ptr, _rhs_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def Solver():
+    from nexd_b200.solver import Solver as S
+    return S
+
+
+@pytest.mark.parametrize("N", [4])
+@pytest.mark.parametrize("kind", ["elastic", "anelastic", "pml", "anelastic_pml"])
+def test_tc_single_rhs_matches_oracle(tmp_path, oracle, Solver, kind, N):
+    """One forward-Euler step from random q, theta and NPML auxiliaries: the
+    tensor-core stage's (x1 - x0)/dt equals the oracle's L(x0)."""
+    m = _rhs_case(tmp_path, kind, N)
+    rng = np.random.default_rng(10 + N)
+    ng = m.K * m.Np
+    qs = np.array([1.2e7] * 6 + [1.0] * 3)
+    q0 = np.asfortranarray((rng.standard_normal((ng, 9)) * qs).astype(np.float32))
+    att, pml = m.desc.attenuation == 1, m.desc.set_pml == 1
+    nth = 6 * m.desc.nMB
+    th0 = np.asfortranarray((rng.standard_normal((ng, nth)) * 1e-4).astype(np.float32)) if att else None
+    aux0 = None
+    if pml:
+        fs = np.array([3e10] * 6 + [4e3] * 3)
+        aux0 = np.asfortranarray((rng.standard_normal((ng, 27)) * np.tile(fs, 3)).astype(np.float32))
+        aux0[np.repeat(m.array("pmlcheck") == 0, m.Np)] = 0.0
+    s = Solver(m.desc_ptr)
+    s.set_contraction("bf16x3")
+    s.set_field(q0)
+    if att:
+        s.set_state(th0, _abi.NEXD_STATE_THETA)
+    if pml:
+        s.set_state(aux0, _abi.NEXD_STATE_PML)
+    s.run(1, 1)
+    dt = np.float32(m.dt)
+    rq = np.zeros((ng, 9), order="F")
+    arq = np.zeros((ng, nth), order="F") if att else None
+    auxr = np.zeros((ng, 27), order="F") if pml else None
+    f64 = lambda a: None if a is None else np.asfortranarray(a.astype(np.float64))
+    assert oracle.oracle_rhs(m.desc_ptr, 64, 1, 0, _ptr(f64(q0)), _ptr(f64(th0)), _ptr(f64(aux0)), _ptr(rq),
+                             _ptr(arq), _ptr(auxr)) == 0
+    checks = [("q", q0, s.field(), rq)]
+    if att:
+        checks.append(("theta", th0, s.state(_abi.NEXD_STATE_THETA, nfields=nth), arq))
+    if pml:
+        checks.append(("aux", aux0, s.state(_abi.NEXD_STATE_PML, nfields=27), auxr))
+    for name, x0, x1, ref in checks:
+        got = (x1.astype(np.float64) - x0.astype(np.float64)) / dt
+        err = rel_l2(got, ref)
+        tol = 2e-5 + 8 * np.finfo(np.float32).eps * np.linalg.norm(x0) / (m.dt * np.linalg.norm(ref))
+        assert err < tol, (kind, N, name, err, tol)
+
+
+def test_tc_cube_traces(tmp_path, oracle, Solver):
+    """Elastic cube (6,000 tets at N=4, LSERK4, 400 steps): tensor-core traces
+    within 1e-4 of the FP64 oracle."""
+    d = str(tmp_path / "cube")
+    synth.write_cube(d, nt=400)
+    m = Mesh(d, N=4, stf_stage_time=True)
+    s = Solver(m.desc_ptr)
+    s.set_contraction("bf16x3")
+    s.run(1, 400)
+    to = run_oracle(oracle, m, 64)[..., 0]
+    assert np.abs(to).max() > 1e-12
+    assert trace_misfit(s.traces()[..., 0], to) < 1e-4
+
+
+def test_tc_twolayer_anelastic_pml_traces(tmp_path, oracle, Solver):
+    """Two-layer Zener + NPML model (N=4, 3,000 tets, LSERK4, 150 steps):
+    tensor-core traces and final wavefield within 1e-4 of the FP64 oracle."""
+    d = str(tmp_path / "tl")
+    synth.write_twolayer(d, cells=(10, 10, 5), nt=150, nrec=12, src_depth=(900.0, 900.0))
+    m = Mesh(d, N=4, stf_stage_time=True)
+    s = Solver(m.desc_ptr)
+    s.set_contraction("bf16x3")
+    s.run(1, 150)
+    to, fo = run_oracle(oracle, m, 64, want_field=True)
+    assert trace_misfit(s.traces()[..., 0], to[..., 0]) < 1e-4
+    assert rel_l2(s.field(), fo[..., 0]) < 1e-4
+
+
+@pytest.mark.parametrize("timeint", [2, 3])
+def test_tc_reference_integrators(tmp_path, oracle, Solver, timeint):
+    """TVD RK2 / RK3 stage updates with the tensor-core contraction."""
+    d = str(tmp_path / f"ti{timeint}")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=60, nrec=5, src_depth=(800.0, 800.0))
+    m = Mesh(d, N=4, timeint=timeint, cfl=0.3)
+    s = Solver(m.desc_ptr)
+    s.set_contraction("bf16x3")
+    s.run(1, 60)
+    assert trace_misfit(s.traces()[..., 0], run_oracle(oracle, m, 64)[..., 0]) < 1e-4
+
+
+def test_tc_batched_and_switching(tmp_path, Solver):
+    """Batched wavefields on the tensor cores equal single-wavefield runs of
+    the same path; switching the contraction mid-run keeps the state."""
+    d = str(tmp_path / "b")
+    synth.write_twolayer(d, cells=(8, 8, 4), nt=60, nrec=4, nsrc=2, src_depth=(700.0, 1200.0))
+    mb = Mesh(d, N=4, nbatch=2, stf_stage_time=True)
+    sb = Solver(mb.desc_ptr)
+    sb.set_contraction("bf16x3")
+    sb.run(1, 60)
+    tb = sb.traces()
+    for b in range(2):
+        ms = Mesh(d, N=4, nbatch=2, stf_stage_time=True)
+        stf = ms.array("stf")
+        stf[:, :, 1 - b] = 0.0
+        ss = Solver(ms.desc_ptr)
+        ss.set_contraction("bf16x3")
+        ss.run(1, 30)
+        ss.set_contraction("fp32")
+        ss.set_contraction("bf16x3")
+        ss.run(31, 60)
+        assert rel_l2(tb[..., b], ss.traces()[..., b]) < 1e-6
+    # the two contractions agree to the split-product accuracy
+    sf = Solver(mb.desc_ptr)
+    sf.run(1, 60)
+    assert trace_misfit(sf.traces()[..., 0], tb[..., 0]) < 1e-4
+
+
+def test_tc_contraction_errors(tmp_path, Solver):
+    d = str(tmp_path / "c")
+    synth.write_cube(d, cells=3, nt=4)
+    m = Mesh(d, N=3)  # keeps the descriptor's arrays alive while the solver is created
+    s = Solver(m.desc_ptr)
+    with pytest.raises(NexdError) as ei:
+        s.set_contraction("bf16x3")
+    assert ei.value.status == _abi.NEXD_ERR_UNSUPPORTED
+    with pytest.raises(NexdError) as ei:
+        s.set_contraction(7)
+    assert ei.value.status == _abi.NEXD_ERR_INVALID
+    s.run(1, 4)  # still runs on the FP32 path
