@@ -181,8 +181,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--contraction", default="fp32", choices=["fp32", "bf16x3"],
-                    help="element contraction: FP32 CUDA cores or split-BF16 tcgen05 tensor cores")
+    ap.add_argument("--contraction", default="fp32", choices=["fp32", "bf16x3", "auto"],
+                    help="element contraction: FP32 CUDA cores, split-BF16 tcgen05 tensor cores, or the faster "
+                         "per element class (timed before the run)")
     ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
     ap.add_argument("--cells", default=None, help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
     args = ap.parse_args()
@@ -295,7 +296,8 @@ def main():
             "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded two-layer model, per-rank seeded source)",
             "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
-                       "integrator": "LSERK4 (5 stages)", "contraction": args.contraction, "pml_tets": int(prof["stage_pml"]["elements"]),
+                       "integrator": "LSERK4 (5 stages)", "contraction": args.contraction,
+                       "kernels_per_class": s.contraction()[0], "pml_tets": int(prof["stage_pml"]["elements"]),
                        "receivers": nrec, "sources_per_rank": nsrc, "wavefields_per_rank": nb,
                        "timed": "CUDA graphs of two steps; roofline from a per-launch-event pass of K more steps",
                        "l2": f"inputs larger than L2: {state_gb:.1f} GB of state streamed per stage",

@@ -238,12 +238,22 @@ typedef struct nexd_profile {
  * arithmetic (src/timeloopMod.f90:407-465 in FP32); NEXD_CONTRACT_BF16X3 the
  * stacked [Dr Ds Dt LIFT] contraction on the tensor cores (tcgen05) with both
  * operands split three ways into BF16 parts (h + m + l, 24 significant bits)
- * and the six products above 2^-24 accumulated in FP32, order 4
+ * and the six products above 2^-24 accumulated in FP32; order 4
  * (NEXD_ERR_UNSUPPORTED otherwise).  The state, the stage update and
  * everything else stay FP32.  No counterpart in the reference (its loop is
- * FP32 matvecs). */
-enum nexd_contraction { NEXD_CONTRACT_FP32 = 0, NEXD_CONTRACT_BF16X3 = 1 };
+ * FP32 matvecs).
+ * NEXD_CONTRACT_AUTO times both kernels on this mesh (a few stage launches
+ * at the current step boundary that leave the live state unchanged) and keeps
+ * the faster one per element class (NPML elements, the rest); results of the
+ * two agree to FP32 rounding, not bit for bit. */
+enum nexd_contraction { NEXD_CONTRACT_FP32 = 0, NEXD_CONTRACT_BF16X3 = 1, NEXD_CONTRACT_AUTO = 2 };
 int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
+
+/* The kernel kind in use per element class (kinds[0] NPML elements, kinds[1]
+ * the rest: NEXD_CONTRACT_FP32 or NEXD_CONTRACT_BF16X3) and, after an AUTO
+ * selection, the measured ms per stage launch tune_ms[class * 2 + kind]
+ * (0 where not measured).  Either pointer may be NULL. */
+int nexd_get_contraction(const nexd_ctx* ctx, int32_t* kinds, float* tune_ms);
 
 /* Timing of nexd_run with CUDA events on the library's stream, counters reset:
  * on = 0 off; 1 per-launch events per kernel kind plus the run span (steps are

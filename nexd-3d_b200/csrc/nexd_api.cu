@@ -99,7 +99,9 @@ struct nexd_ctx {
   bool use_graphs = true;
   // element contraction: NEXD_CONTRACT_FP32 (CUDA cores) or NEXD_CONTRACT_BF16X3 (tensor cores)
   int contraction = NEXD_CONTRACT_FP32;
-  uint4* ops_tc = nullptr;     // packed operator of the tensor-core kernels (orders 3 and 4)
+  int kind[2] = {NEXD_CONTRACT_FP32, NEXD_CONTRACT_FP32};  // kernel per element class: [0] NPML, [1] the rest
+  float tune_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};           // autotune: [class][kind] ms per launch
+  uint4* ops_tc = nullptr;     // packed operator of the tensor-core kernels (order 4)
 };
 
 namespace {
@@ -211,10 +213,12 @@ TcKernelFn pick_tc_kernel(int N, bool att, bool pml, int mode, size_t& smem) {
 }
 
 // The stacked operator [Dr Ds Dt LIFT] of the tensor-core stage kernel as bf16
-// h, m, l rows (row n' = output node, K-major, 128-byte swizzle): entry
+// H, M, L rows (row n' = output node, K-major, 128-byte swizzle): entry
 // (n', d Np + k) = D_d(n', k), entry (n', KV16 + f NpF + i) = LIFT(n', f NpF + i),
-// zero elsewhere; x = h + m + l with m = bf16(x - h), l = bf16(x - h - m) of
-// the FP64 value.
+// zero elsewhere; x = H + M + L with M = bf16(x - H), L = bf16(x - H - M) of
+// the FP64 value.  (A two-part operator, a fixed 2^-17 relative change, moves
+// the acceleration traces by ~1e-3: the derivative of a smooth field cancels
+// about two digits of its terms.)
 template <int N>
 std::vector<uint16_t> pack_tc_operator(const nexd_desc* d) {
   using T = TcOrder<N>;
@@ -327,7 +331,7 @@ int configure_launch(nexd_ctx* c) {
     const bool pmlk = which == 0;
     size_t smem = 0;
     const void* fn;
-    if (c->contraction == NEXD_CONTRACT_BF16X3) fn = reinterpret_cast<const void*>(pick_tc_kernel(c->N, c->att, pmlk, mode, smem));
+    if (c->kind[which] == NEXD_CONTRACT_BF16X3) fn = reinterpret_cast<const void*>(pick_tc_kernel(c->N, c->att, pmlk, mode, smem));
     else fn = reinterpret_cast<const void*>(pick_kernel(c->N, c->att, pmlk, mode, smem));
     if (!fn) return set_err(c, NEXD_ERR_UNSUPPORTED, "no stage kernel for this order and contraction");
     CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -696,14 +700,27 @@ __global__ void set_step_kernel(int* it_dev, int it) {
 
 // Enqueues `nsteps` steps on the context's stream; the step number comes from
 // the device counter (set before, advanced by tick_kernel after each step).
-void enqueue_body(nexd_ctx* c, int nsteps) {
+// Launches the stage kernel of one element class (NPML elements first in the
+// internal order, then the rest) with the kernel kind chosen for it.
+void launch_class(nexd_ctx* c, StageArgs& a, bool pml) {
   const int mode = c->timeint == 4 ? MODE_LSERK : MODE_TVD;
-  size_t smem_p = 0, smem_m = 0;
-  const bool tcm = c->contraction == NEXD_CONTRACT_BF16X3;
-  KernelFn kp = tcm ? nullptr : pick_kernel(c->N, c->att, true, mode, smem_p);
-  KernelFn km = tcm ? nullptr : pick_kernel(c->N, c->att, false, mode, smem_m);
-  TcKernelFn tp = tcm ? pick_tc_kernel(c->N, c->att, true, mode, smem_p) : nullptr;
-  TcKernelFn tm = tcm ? pick_tc_kernel(c->N, c->att, false, mode, smem_m) : nullptr;
+  const int cls = pml ? 0 : 1;
+  size_t smem = 0;
+  a.e_begin = pml ? 0 : c->Kpml;
+  a.e_end = pml ? c->Kpml : c->K;
+  const int grid = pml ? c->grid_pml : c->grid_main;
+  const size_t sm = pml ? c->smem_pml : c->smem_main;
+  if (c->kind[cls] == NEXD_CONTRACT_BF16X3) {
+    TcKernelFn f = pick_tc_kernel(c->N, c->att, pml, mode, smem);
+    f<<<grid, 256, sm, c->stream>>>(a, c->ops_tc);
+  } else {
+    KernelFn f = pick_kernel(c->N, c->att, pml, mode, smem);
+    f<<<grid, 256, sm, c->stream>>>(a);
+  }
+}
+
+// Stage arguments that do not change from stage to stage.
+StageArgs base_args(nexd_ctx* c) {
   StageArgs a{};
   a.flag = c->flag;
   a.nbatch = c->nbatch;
@@ -739,6 +756,11 @@ void enqueue_body(nexd_ctx* c, int nsteps) {
   a.abuf = c->abuf;
   a.nslot = std::max(1, c->nslot);
   a.pml_off = c->pml_off;
+  return a;
+}
+
+void enqueue_body(nexd_ctx* c, int nsteps) {
+  StageArgs a = base_args(c);
   RecordArgs r{};
   r.nrec = c->nrec;
   r.nbatch = c->nbatch;
@@ -794,20 +816,14 @@ void enqueue_body(nexd_ctx* c, int nsteps) {
       a.q_out = c->qbuf[outb];
       a.q_n = qn;
       if (c->Kpml > 0) {
-        a.e_begin = 0;
-        a.e_end = c->Kpml;
         const int ev = ev_begin(c, NEXD_K_STAGE_PML);
-        if (tcm) tp<<<c->grid_pml, 256, c->smem_pml, c->stream>>>(a, c->ops_tc);
-        else kp<<<c->grid_pml, 256, c->smem_pml, c->stream>>>(a);
+        launch_class(c, a, true);
         ev_end(c, ev);
         ++c->launches;
       }
       if (c->K > c->Kpml) {
-        a.e_begin = c->Kpml;
-        a.e_end = c->K;
         const int ev = ev_begin(c, NEXD_K_STAGE_MAIN);
-        if (tcm) tm<<<c->grid_main, 256, c->smem_main, c->stream>>>(a, c->ops_tc);
-        else km<<<c->grid_main, 256, c->smem_main, c->stream>>>(a);
+        launch_class(c, a, false);
         ev_end(c, ev);
         ++c->launches;
       }
@@ -960,21 +976,98 @@ int nexd_step_io(nexd_ctx* c, int32_t it, const float* stf_in, float* traces_out
   return NEXD_OK;
 }
 
+namespace {
+
+// Times `reps` launches of one class's stage kernel with the current kind.
+// The launches are first stages with cb = 0 (LSERK: ca = 0; TVD: ca = 1) and
+// no receiver capture: they rewrite only the residuals, the step-start copies
+// and the other wavefield buffer, which the next first stage rewrites anyway,
+// and leave theta, the NPML auxiliaries and the current wavefield as they
+// were.  The step counter is set to a valid step for the source lookup (every
+// run sets it again).
+int time_class(nexd_ctx* c, bool pml, int reps, float& ms) {
+  StageArgs a = base_args(c);
+  a.stage = 0;
+  a.stage_first = 1;
+  a.last_stage = 0;
+  a.ca = c->timeint == 4 ? 0.f : 1.f;
+  a.cb = 0.f;
+  set_step_kernel<<<1, 32, 0, c->stream>>>(c->it_dev, 1);
+  a.q_in = c->qbuf[c->cur];
+  a.q_out = c->qbuf[(c->cur + 1) % (c->timeint == 3 ? 3 : 2)];
+  a.q_n = c->qbuf[c->cur];
+  cudaEvent_t e0, e1;
+  CUDA_TRY(c, cudaEventCreate(&e0));
+  CUDA_TRY(c, cudaEventCreate(&e1));
+  launch_class(c, a, pml);  // warm-up
+  CUDA_TRY(c, cudaEventRecord(e0, c->stream));
+  for (int i = 0; i < reps; ++i) launch_class(c, a, pml);
+  CUDA_TRY(c, cudaEventRecord(e1, c->stream));
+  CUDA_TRY(c, cudaEventSynchronize(e1));
+  CUDA_TRY(c, cudaGetLastError());
+  float t = 0.f;
+  CUDA_TRY(c, cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ms = t / float(reps);
+  return NEXD_OK;
+}
+
+// Picks, per element class, the faster of the FP32 CUDA-core kernel and the
+// tensor-core kernel on this mesh (both FP32-accurate; results of the two
+// agree to FP32 rounding, not bit for bit).
+int autotune(nexd_ctx* c) {
+  if (int st = finish(c)) return st;  // at a step boundary
+  for (int cls = 0; cls < 2; ++cls) {
+    const int nel = cls == 0 ? c->Kpml : c->K - c->Kpml;
+    if (nel == 0) continue;
+    int best = NEXD_CONTRACT_FP32;
+    for (int k = 0; k < 2; ++k) {
+      c->kind[cls] = k;
+      if (int st = configure_launch(c)) return st;
+      if (int st = time_class(c, cls == 0, 3, c->tune_ms[cls][k])) return st;
+      if (c->tune_ms[cls][k] < c->tune_ms[cls][best]) best = k;
+    }
+    c->kind[cls] = best;
+  }
+  return configure_launch(c);
+}
+
+}  // namespace
+
 int nexd_set_contraction(nexd_ctx* c, int32_t mode) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
-  if (mode != NEXD_CONTRACT_FP32 && mode != NEXD_CONTRACT_BF16X3)
+  if (mode != NEXD_CONTRACT_FP32 && mode != NEXD_CONTRACT_BF16X3 && mode != NEXD_CONTRACT_AUTO)
     return set_err(c, NEXD_ERR_INVALID, "unknown contraction mode");
-  if (mode == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N))
+  if (mode != NEXD_CONTRACT_FP32 && !tc_order_supported(c->N))
     return set_err(c, NEXD_ERR_UNSUPPORTED, "the tensor-core contraction covers order 4");
-  if (mode == c->contraction) return NEXD_OK;
-  const int old = c->contraction;
-  c->contraction = mode;
-  if (int st = configure_launch(c)) {
-    c->contraction = old;
+  const int old[2] = {c->kind[0], c->kind[1]};
+  int st;
+  if (mode == NEXD_CONTRACT_AUTO) {
+    st = autotune(c);
+  } else {
+    c->kind[0] = c->kind[1] = mode;
+    st = configure_launch(c);
+  }
+  if (st) {
+    c->kind[0] = old[0];
+    c->kind[1] = old[1];
     configure_launch(c);
     return st;
   }
+  c->contraction = mode;
   drop_graphs(c);
+  return NEXD_OK;
+}
+
+int nexd_get_contraction(const nexd_ctx* c, int32_t* kinds, float* tune_ms) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (kinds) {
+    kinds[0] = c->kind[0];
+    kinds[1] = c->kind[1];
+  }
+  if (tune_ms)
+    for (int i = 0; i < 4; ++i) tune_ms[i] = c->tune_ms[i / 2][i % 2];
   return NEXD_OK;
 }
 

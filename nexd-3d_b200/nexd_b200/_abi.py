@@ -63,7 +63,7 @@ HOST_SYMBOLS = ["nexd_mesh_build", "nexd_mesh_desc", "nexd_mesh_get_info", "nexd
                 "nexd_mesh_last_error", "nexd_mesh_free"]
 GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
                "nexd_get_state", "nexd_set_state", "nexd_step_io", "nexd_pml_trigger", "nexd_get_energy",
-               "nexd_set_contraction",
+               "nexd_set_contraction", "nexd_get_contraction",
                "nexd_wavefield_energy_noalloc", "nexd_profile_enable", "nexd_profile_get",
                "nexd_last_error", "nexd_launch_count", "nexd_destroy"]
 NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_ENERGY, NEXD_K_COUNT = 0, 1, 2, 3, 4
@@ -74,7 +74,7 @@ class NexdProfile(C.Structure):
                 ("elements", C.c_int64 * NEXD_K_COUNT), ("span_ms", C.c_double)]
 NEXD_STATE_Q, NEXD_STATE_THETA, NEXD_STATE_PML = 0, 1, 2
 NEXD_NOALLOC_MAX_BATCH = 64
-NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3 = 0, 1
+NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3, NEXD_CONTRACT_AUTO = 0, 1, 2
 
 _host = None
 _gpu = None
@@ -124,6 +124,7 @@ def gpu_lib():
         lib.nexd_pml_trigger.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_int32]
         lib.nexd_get_energy.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.nexd_set_contraction.argtypes = [vp, C.c_int32]
+        lib.nexd_get_contraction.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
         lib.nexd_wavefield_energy_noalloc.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32,
                                                       C.POINTER(C.c_double)]
         lib.nexd_profile_enable.argtypes = [vp, C.c_int32]

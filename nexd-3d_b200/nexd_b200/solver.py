@@ -90,12 +90,25 @@ class Solver:
         return out
 
     def set_contraction(self, mode):
-        """Element contraction arithmetic: "fp32" (CUDA cores, default) or
-        "bf16x3" (tcgen05 tensor cores, split BF16, FP32 accumulation)."""
-        m = {"fp32": _abi.NEXD_CONTRACT_FP32, "bf16x3": _abi.NEXD_CONTRACT_BF16X3}.get(mode, mode)
+        """Element contraction arithmetic: "fp32" (CUDA cores, default),
+        "bf16x3" (tcgen05 tensor cores, split BF16, FP32 accumulation) or
+        "auto" (the faster of the two per element class, timed on this mesh)."""
+        m = {"fp32": _abi.NEXD_CONTRACT_FP32, "bf16x3": _abi.NEXD_CONTRACT_BF16X3,
+             "auto": _abi.NEXD_CONTRACT_AUTO}.get(mode, mode)
         st = _abi.gpu_lib().nexd_set_contraction(self._ctx, m)
         if st != 0:
             raise _gpu_error(self._ctx, st)
+
+    def contraction(self):
+        """({"npml": kind, "rest": kind}, autotune ms per launch {(class, kind): ms})."""
+        kinds = (C.c_int32 * 2)()
+        ms = (C.c_float * 4)()
+        st = _abi.gpu_lib().nexd_get_contraction(self._ctx, kinds, ms)
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+        names = {0: "fp32", 1: "bf16x3"}
+        return ({"npml": names[kinds[0]], "rest": names[kinds[1]]},
+                {(cl, names[k]): ms[2 * i + k] for i, cl in enumerate(("npml", "rest")) for k in range(2)})
 
     def pml_trigger(self, avg_window1=10, avg_window2=2, sta_lta_trigger=0.1, f0=1.0, formula=0):
         """Arm the NPML energy STA/LTA trigger (src/timeloopMod.f90:508-542)."""

@@ -1,5 +1,5 @@
 """The tensor-core contraction (NEXD_CONTRACT_BF16X3: tcgen05, both operands
-split three ways into BF16 parts, six products accumulated in FP32) against
+split three ways into BF16 parts, six products accumulated in FP32) and the per-class autotune (NEXD_CONTRACT_AUTO) against
 the FP64 oracle and against the FP32 CUDA-core path, through the C-ABI.
 
 Tolerances are those of the FP32 path: one right-hand side within 2e-5
@@ -150,3 +150,26 @@ def test_tc_contraction_errors(tmp_path, Solver):
         s.set_contraction(7)
     assert ei.value.status == _abi.NEXD_ERR_INVALID
     s.run(1, 4)  # still runs on the FP32 path
+
+
+@pytest.mark.parametrize("timeint", [4, 2])
+def test_autotune_leaves_state_and_picks_valid_kinds(tmp_path, oracle, Solver, timeint):
+    """The autotune's timing launches at a step boundary leave the wavefield,
+    memory variables and NPML auxiliaries bit-identical; the run continues on
+    the chosen kernels within the FP32 tolerance of the oracle."""
+    d = str(tmp_path / "auto")
+    synth.write_twolayer(d, cells=(8, 8, 4), nt=60, nrec=6, src_depth=(900.0, 900.0))
+    m = Mesh(d, N=4, timeint=timeint, stf_stage_time=(timeint == 4), cfl=0.3)
+    s = Solver(m.desc_ptr)
+    s.run(1, 30)
+    nth = 6 * m.desc.nMB
+    before = (s.field(), s.state(_abi.NEXD_STATE_THETA, nfields=nth), s.state(_abi.NEXD_STATE_PML, nfields=27))
+    s.set_contraction("auto")
+    after = (s.field(), s.state(_abi.NEXD_STATE_THETA, nfields=nth), s.state(_abi.NEXD_STATE_PML, nfields=27))
+    for x, y in zip(before, after):
+        assert np.array_equal(x, y)
+    kinds, ms = s.contraction()
+    assert set(kinds.values()) <= {"fp32", "bf16x3"}
+    assert all(v > 0 for v in ms.values())
+    s.run(31, 60)
+    assert trace_misfit(s.traces()[..., 0], run_oracle(oracle, m, 64)[..., 0]) < 1e-4
