@@ -223,7 +223,8 @@ enum nexd_kernel_kind {
   NEXD_K_STAGE_PML = 1,
   NEXD_K_STAGE_MAIN = 2,
   NEXD_K_ENERGY = 3,
-  NEXD_K_COUNT = 4
+  NEXD_K_BOUNDARY = 4,  /* learned-boundary ghost states */
+  NEXD_K_COUNT = 5
 };
 
 typedef struct nexd_profile {
@@ -254,6 +255,55 @@ int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
  * selection, the measured ms per stage launch tune_ms[class * 2 + kind]
  * (0 where not measured).  Either pointer may be NULL. */
 int nexd_get_contraction(const nexd_ctx* ctx, int32_t* kinds, float* tune_ms);
+
+/* ---- Learned absorbing boundary (no counterpart in the reference) ----------
+ * Absorbing faces (face code -2) normally take the exterior state as zero
+ * (computeExactRiemannSF with -VT, src/waveMod.f90:269-336).  The upwind flux
+ * sees the exterior state only through the incoming characteristic values
+ * w = (n.S.n - Zp v.n, n.S.s - Zs v.s, n.S.t - Zs v.t) per face node (n the
+ * outward normal, s, t the face tangents, Zp = rho vp, Zs = rho vs).  With a
+ * boundary MLP set, every stage first predicts the exterior state of each
+ * absorbing face from its interior trace: features per face node in the face
+ * frame (v.n, v.s, v.t, n.S.n, n.S.s, n.S.t, s.S.s, t.S.t, s.S.t) with the
+ * stresses divided by Zp, ordered node-major (feature index = 9 * face node +
+ * component) in the element's own face-node order, the vector divided by its
+ * RMS value r; network 9 NpF -> 128 -> 128 -> 9 NpF with GELU, applied with
+ * BF16 weights and FP32 accumulation; the prediction (same units, times r)
+ * gives w, clamped to |w| <= max_reflection |u| with u = (n.S.n + Zp v.n,
+ * ...) the interior's outgoing values, so the boundary stays dissipative.
+ * max_reflection = 0, or a network whose last layer is zero, reproduces the
+ * plain absorbing boundary exactly. */
+
+/* Absorbing faces in ghost-slot order: count, and (either may be NULL) the
+ * 1-based element and face (1..4) of each. */
+int nexd_boundary_faces(const nexd_ctx* ctx, int32_t* nbf, int32_t* elem, int32_t* face);
+/* Sets the boundary MLP from FP32 parameters (host memory, count =
+ * nexd_mlp_param_count(9 NpF, 128), layout [W1 (128 x 9NpF), b1, W2 (128 x 128),
+ * b2, W3 (9NpF x 128), b3] row-major) and the reflection bound in [0, 1);
+ * params NULL switches back to the plain absorbing boundary. */
+int nexd_set_boundary_mlp(nexd_ctx* ctx, const float* params, int64_t count, float max_reflection);
+/* The exterior states of the last stage (traction w_P n + w_S1 s + w_S2 t as a
+ * stress, zero velocity): (NpF, 9, nbf, nbatch) floats. */
+int nexd_get_ghost(nexd_ctx* ctx, float* out);
+/* Face traces of the current wavefield for faces (elem 1-based, face 1..4):
+ * out (NpF, 9, 2, nfaces, nbatch) floats, side 1 = the element's own trace,
+ * side 2 = the neighbour's (zero on boundary faces), both in the element's
+ * own face-node order.  Used to record training pairs from wide-NPML runs. */
+int nexd_get_face_traces(nexd_ctx* ctx, int32_t nfaces, const int32_t* elem, const int32_t* face, float* out);
+
+/* MLP training kernels (FP32; every pointer is device memory owned by the
+ * caller; stream may be NULL).  Network n_in -> n_hidden -> n_hidden -> n_in,
+ * GELU, parameters as above; work holds nexd_mlp_workspace_floats floats.
+ * nexd_mlp_loss_grad: loss = mean over the batch of |y - target|^2 (summed
+ * over outputs), written to *loss (device), and its gradient. */
+int64_t nexd_mlp_param_count(int32_t n_in, int32_t n_hidden);
+int64_t nexd_mlp_workspace_floats(int32_t n_in, int32_t n_hidden, int32_t batch);
+int nexd_mlp_forward(int32_t n_in, int32_t n_hidden, const float* params, const float* x, int32_t batch, float* y,
+                     float* work, void* stream);
+int nexd_mlp_loss_grad(int32_t n_in, int32_t n_hidden, const float* params, const float* x, const float* target,
+                       int32_t batch, float* grads, float* loss, float* work, void* stream);
+int nexd_mlp_adam(int64_t count, float* params, const float* grads, float* m, float* v, int32_t step, float lr,
+                  float beta1, float beta2, float eps, void* stream);
 
 /* Timing of nexd_run with CUDA events on the library's stream, counters reset:
  * on = 0 off; 1 per-launch events per kernel kind plus the run span (steps are

@@ -18,6 +18,7 @@
 #include "energy_kernel.cuh"
 #include "stage_kernel.cuh"
 #include "stage_tc.cuh"
+#include "boundary_mlp.cuh"
 
 using namespace nexd_dev;
 
@@ -102,6 +103,20 @@ struct nexd_ctx {
   int kind[2] = {NEXD_CONTRACT_FP32, NEXD_CONTRACT_FP32};  // kernel per element class: [0] NPML, [1] the rest
   float tune_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};           // autotune: [class][kind] ms per launch
   uint4* ops_tc = nullptr;     // packed operator of the tensor-core kernels (order 4)
+  // learned absorbing boundary: absorbing faces, their ghost states and the MLP
+  int nbf = 0;                       // absorbing faces
+  int *bf_elem = nullptr, *bf_face = nullptr;  // [nbf] internal element, local face
+  int4* fcode_learned = nullptr;     // face codes with absorbing faces as -3 - ghost index
+  float* ghost = nullptr;            // [nbatch][nbf][9][NpF]
+  __nv_bfloat16* mlp_w = nullptr;    // parameters in bf16
+  float* mlp_stage = nullptr;        // FP32 upload buffer of the parameters
+  bool mlp_on = false;
+  float mlp_rho = 0.f;               // bound of the incoming / outgoing characteristic ratio
+  int ghost_grid = 0;
+  size_t ghost_smem = 0;
+  int* gather_idx = nullptr;         // face-trace gather scratch
+  float* gather_out = nullptr;
+  int gather_cap = 0;
 };
 
 namespace {
@@ -561,6 +576,22 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
       fc4[i] = make_int4(h_fcode[4 * i], h_fcode[4 * i + 1], h_fcode[4 * i + 2], h_fcode[4 * i + 3]);
     }
     if ((st = upload(c, &c->nbr, nb4)) || (st = upload(c, &c->fcode, fc4))) return fail(st);
+    // absorbing faces in internal element order: the learned boundary's ghost slots
+    std::vector<int> bfe, bff;
+    std::vector<int4> fl4 = fc4;
+    for (int i = 0; i < K; ++i) {
+      int* cs = reinterpret_cast<int*>(&fl4[i]);
+      for (int f = 0; f < 4; ++f)
+        if (cs[f] == -2) {
+          cs[f] = -3 - int(bfe.size());
+          bfe.push_back(i);
+          bff.push_back(f);
+        }
+    }
+    c->nbf = int(bfe.size());
+    if (c->nbf > 0 &&
+        ((st = upload(c, &c->bf_elem, bfe)) || (st = upload(c, &c->bf_face, bff)) || (st = upload(c, &c->fcode_learned, fl4))))
+      return fail(st);
   }
   const int nq = (c->timeint == 3) ? 3 : 2;
   for (int i = 0; i < nq; ++i) {
@@ -732,7 +763,9 @@ StageArgs base_args(nexd_ctx* c) {
   a.L = c->L;
   a.geo = c->geo;
   a.nbr = c->nbr;
-  a.fcode = c->fcode;
+  a.fcode = c->mlp_on ? c->fcode_learned : c->fcode;
+  a.ghost = c->mlp_on ? c->ghost : nullptr;
+  a.nbf = c->nbf;
   a.patterns = c->patterns;
   a.npat = c->npat;
   a.ael = c->ael;
@@ -815,6 +848,27 @@ void enqueue_body(nexd_ctx* c, int nsteps) {
       a.q_in = c->qbuf[in];
       a.q_out = c->qbuf[outb];
       a.q_n = qn;
+      if (c->mlp_on) {
+        // exterior states of the absorbing faces from this stage's input
+        GhostArgs ga{};
+        ga.nbf = c->nbf;
+        ga.nbatch = c->nbatch;
+        ga.NpF = c->NpF;
+        ga.Np = c->Np;
+        ga.ldq = c->ldq;
+        ga.q = a.q_in;
+        ga.bf_elem = c->bf_elem;
+        ga.bf_face = c->bf_face;
+        ga.geo = c->geo;
+        ga.pat = c->patterns;
+        ga.w = c->mlp_w;
+        ga.rho_max = c->mlp_rho;
+        ga.ghost = c->ghost;
+        const int ev = ev_begin(c, NEXD_K_BOUNDARY);
+        ghost_kernel<<<c->ghost_grid, kGhostThreads, c->ghost_smem, c->stream>>>(ga);
+        ev_end(c, ev);
+        ++c->launches;
+      }
       if (c->Kpml > 0) {
         const int ev = ev_begin(c, NEXD_K_STAGE_PML);
         launch_class(c, a, true);
@@ -1112,6 +1166,251 @@ int nexd_get_energy(nexd_ctx* c, double* energy, int32_t* pml_switch) {
     CUDA_TRY(c, cudaMemcpyAsync(pml_switch, c->pml_switch, c->nbatch * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return NEXD_OK;
+}
+
+// ---- learned absorbing boundary ---------------------------------------------
+
+int nexd_boundary_faces(const nexd_ctx* c, int32_t* nbf, int32_t* elem, int32_t* face) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (nbf) *nbf = c->nbf;
+  if ((elem || face) && c->nbf > 0) {
+    std::vector<int> e(c->nbf), f(c->nbf);
+    CUDA_TRY(const_cast<nexd_ctx*>(c), cudaMemcpy(e.data(), c->bf_elem, c->nbf * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(const_cast<nexd_ctx*>(c), cudaMemcpy(f.data(), c->bf_face, c->nbf * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < c->nbf; ++i) {
+      if (elem) elem[i] = c->new2old[e[i]] + 1;
+      if (face) face[i] = f[i] + 1;
+    }
+  }
+  return NEXD_OK;
+}
+
+int nexd_set_boundary_mlp(nexd_ctx* c, const float* params, int64_t count, float max_reflection) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (!params) {
+    c->mlp_on = false;
+    drop_graphs(c);
+    return NEXD_OK;
+  }
+  if (c->nbf == 0) return set_err(c, NEXD_ERR_UNSUPPORTED, "the mesh has no absorbing faces");
+  const int nin = 9 * c->NpF;
+  if (count != mlp_param_count(nin, kMlpHidden))
+    return set_err(c, NEXD_ERR_INVALID, "parameter count does not match a 9 NpF -> 128 -> 128 -> 9 NpF network");
+  if (!(max_reflection >= 0.f && max_reflection < 1.f))
+    return set_err(c, NEXD_ERR_INVALID, "max_reflection must be in [0, 1)");
+  c->mlp_rho = max_reflection;
+  int st;
+  if (!c->mlp_w) {
+    if ((st = dalloc(c, &c->mlp_stage, size_t(count))) || (st = dalloc(c, &c->mlp_w, size_t(count))) ||
+        (st = dalloc(c, &c->ghost, size_t(c->nbatch) * c->nbf * 9 * c->NpF)))
+      return st;
+    c->ghost_smem = ghost_smem_bytes(nin);
+    CUDA_TRY(c, cudaFuncSetAttribute(ghost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c->ghost_smem)));
+    int per_sm = 0;
+    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ghost_kernel, kGhostThreads, c->ghost_smem));
+    if (per_sm < 1) return set_err(c, NEXD_ERR_UNSUPPORTED, "boundary MLP kernel does not fit on an SM");
+    const long long groups = ((long long)c->nbf * c->nbatch + kGhostFaces - 1) / kGhostFaces;
+    c->ghost_grid = int(std::max<long long>(1, std::min<long long>(groups, (long long)per_sm * c->nsm)));
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(c->mlp_stage, params, size_t(count) * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  to_bf16_kernel<<<unsigned((count + 255) / 256), 256, 0, c->stream>>>(count, c->mlp_stage, c->mlp_w);
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->mlp_on = true;
+  drop_graphs(c);
+  return NEXD_OK;
+}
+
+int nexd_get_ghost(nexd_ctx* c, float* out) {
+  if (!c || !out) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  if (!c->ghost) return set_err(c, NEXD_ERR_INVALID, "no boundary MLP has been set");
+  CUDA_TRY(c, cudaMemcpyAsync(out, c->ghost, size_t(c->nbatch) * c->nbf * 9 * c->NpF * sizeof(float),
+                              cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return NEXD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Face traces of the current wavefield: out[b][i][side][9][NpF], side 0 the
+// element's own trace, side 1 the neighbour's (zero on boundary faces), both
+// in the element's own face-node order.
+__global__ void face_trace_kernel(int nf, int nbatch, int Np, int NpF, long long ldq, const float* q, const int* fe,
+                                  const int* ff, const int4* nbr, const int4* fcode, const unsigned char* pat,
+                                  float* out) {
+  const long long n = (long long)nbatch * nf * NpF;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int fi = int(t % NpF);
+    const long long bi = t / NpF;
+    const int i = int(bi % nf), b = int(bi / nf);
+    const int e = fe[i], f = ff[i];
+    const float* qb = q + (long long)b * 9 * ldq;
+    const long long own = (long long)e * Np + pat[f * NpF + fi];
+    const int code = reinterpret_cast<const int*>(fcode)[4 * e + f];
+    float* o = out + bi * 2 * 9 * NpF + fi;
+    for (int c = 0; c < 9; ++c) o[c * NpF] = qb[c * ldq + own];
+    if (code >= 0) {
+      const int nb = reinterpret_cast<const int*>(nbr)[4 * e + f];
+      const long long other = (long long)nb * Np + pat[code * NpF + fi];
+      for (int c = 0; c < 9; ++c) o[(9 + c) * NpF] = qb[c * ldq + other];
+    } else {
+      for (int c = 0; c < 9; ++c) o[(9 + c) * NpF] = 0.f;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int nexd_get_face_traces(nexd_ctx* c, int32_t nfaces, const int32_t* elem, const int32_t* face, float* out) {
+  if (!c || nfaces < 0 || (nfaces > 0 && (!elem || !face || !out))) return set_err(c, NEXD_ERR_INVALID, "bad arguments");
+  if (nfaces == 0) return NEXD_OK;
+  std::vector<int> idx(size_t(2) * nfaces);
+  for (int i = 0; i < nfaces; ++i) {
+    if (elem[i] < 1 || elem[i] > c->K || face[i] < 1 || face[i] > 4)
+      return set_err(c, NEXD_ERR_INVALID, "face index out of range");
+    idx[i] = c->old2new[elem[i] - 1];
+    idx[nfaces + i] = face[i] - 1;
+  }
+  const size_t nout = size_t(c->nbatch) * nfaces * 2 * 9 * c->NpF;
+  if (nfaces > c->gather_cap) {
+    int st;
+    if ((st = dalloc(c, &c->gather_idx, idx.size())) || (st = dalloc(c, &c->gather_out, nout))) return st;
+    c->gather_cap = nfaces;
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(c->gather_idx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  const long long items = (long long)c->nbatch * nfaces * c->NpF;
+  face_trace_kernel<<<unsigned(std::min<long long>((items + 255) / 256, 4096)), 256, 0, c->stream>>>(
+      nfaces, c->nbatch, c->Np, c->NpF, c->ldq, c->qbuf[c->cur], c->gather_idx, c->gather_idx + nfaces, c->nbr,
+      c->fcode, c->patterns, c->gather_out);
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaMemcpyAsync(out, c->gather_out, nout * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return NEXD_OK;
+}
+
+// ---- MLP training kernels (device pointers owned by the caller) ----------------
+
+int64_t nexd_mlp_param_count(int32_t n_in, int32_t n_hidden) { return mlp_param_count(n_in, n_hidden); }
+
+int64_t nexd_mlp_workspace_floats(int32_t n_in, int32_t n_hidden, int32_t batch) {
+  return 6LL * batch * n_hidden + 2LL * batch * n_in + 256;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct MlpView {
+  const float *W1, *b1, *W2, *b2, *W3, *b3;
+  float *Z1, *A1, *Z2, *A2, *Y, *dY, *dH1, *dH2, *partial;
+};
+
+MlpView mlp_view(int nin, int H, int B, const float* p, float* work) {
+  MlpView v;
+  v.W1 = p;
+  v.b1 = v.W1 + (long long)H * nin;
+  v.W2 = v.b1 + H;
+  v.b2 = v.W2 + (long long)H * H;
+  v.W3 = v.b2 + H;
+  v.b3 = v.W3 + (long long)nin * H;
+  const long long BH = (long long)B * H, BI = (long long)B * nin;
+  v.Z1 = work;
+  v.A1 = v.Z1 + BH;
+  v.Z2 = v.A1 + BH;
+  v.A2 = v.Z2 + BH;
+  v.Y = v.A2 + BH;
+  v.dY = v.Y + BI;
+  v.dH1 = v.dY + BI;
+  v.dH2 = v.dH1 + BH;
+  v.partial = v.dH2 + BH;
+  return v;
+}
+
+template <bool TA, bool TB>
+void gemm(cudaStream_t s, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc,
+          int acc) {
+  dim3 grid((N + 63) / 64, (M + 63) / 64);
+  gemm_kernel<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, acc);
+}
+
+unsigned blocks_for(long long n) { return unsigned((n + 255) / 256); }
+
+void mlp_forward(cudaStream_t s, int nin, int H, int B, const float* x, const MlpView& v) {
+  gemm<false, true>(s, B, H, nin, x, nin, v.W1, nin, v.Z1, H, 0);
+  bias_act_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>(B, H, v.Z1, v.b1, v.A1, 1);
+  gemm<false, true>(s, B, H, H, v.A1, H, v.W2, H, v.Z2, H, 0);
+  bias_act_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>(B, H, v.Z2, v.b2, v.A2, 1);
+  gemm<false, true>(s, B, nin, H, v.A2, H, v.W3, H, v.Y, nin, 0);
+  bias_act_kernel<<<blocks_for((long long)B * nin), 256, 0, s>>>(B, nin, v.Y, v.b3, v.Y, 0);
+}
+
+int mlp_check(int32_t n_in, int32_t n_hidden, int32_t batch) {
+  if (n_in < 1 || n_hidden < 1 || batch < 1) return set_err(nullptr, NEXD_ERR_INVALID, "bad MLP dimensions");
+  return NEXD_OK;
+}
+
+int mlp_status() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(nullptr, NEXD_ERR_CUDA, std::string("MLP kernel: ") + cudaGetErrorString(e));
+  return NEXD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nexd_mlp_forward(int32_t n_in, int32_t n_hidden, const float* params, const float* x, int32_t batch, float* y,
+                     float* work, void* stream) {
+  if (int st = mlp_check(n_in, n_hidden, batch)) return st;
+  if (!params || !x || !y || !work) return set_err(nullptr, NEXD_ERR_INVALID, "null pointer");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  MlpView v = mlp_view(n_in, n_hidden, batch, params, work);
+  mlp_forward(s, n_in, n_hidden, batch, x, v);
+  cudaMemcpyAsync(y, v.Y, size_t(batch) * n_in * sizeof(float), cudaMemcpyDeviceToDevice, s);
+  return mlp_status();
+}
+
+int nexd_mlp_loss_grad(int32_t n_in, int32_t n_hidden, const float* params, const float* x, const float* target,
+                       int32_t batch, float* grads, float* loss, float* work, void* stream) {
+  if (int st = mlp_check(n_in, n_hidden, batch)) return st;
+  if (!params || !x || !target || !grads || !loss || !work) return set_err(nullptr, NEXD_ERR_INVALID, "null pointer");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int nin = n_in, H = n_hidden, B = batch;
+  MlpView v = mlp_view(nin, H, B, params, work);
+  mlp_forward(s, nin, H, B, x, v);
+  float* gW1 = grads;
+  float* gb1 = gW1 + (long long)H * nin;
+  float* gW2 = gb1 + H;
+  float* gb2 = gW2 + (long long)H * H;
+  float* gW3 = gb2 + H;
+  float* gb3 = gW3 + (long long)nin * H;
+  const long long n = (long long)B * nin;
+  mse_kernel<<<256, 256, 0, s>>>(n, B, v.Y, target, v.dY, v.partial);
+  sum_partials_kernel<<<1, 32, 0, s>>>(256, v.partial, B, loss);
+  gemm<true, false>(s, nin, H, B, v.dY, nin, v.A2, H, gW3, H, 0);
+  colsum_kernel<<<blocks_for(nin), 256, 0, s>>>(B, nin, v.dY, gb3);
+  gemm<false, false>(s, B, H, nin, v.dY, nin, v.W3, H, v.dH2, H, 0);
+  gelu_back_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>((long long)B * H, v.dH2, v.Z2);
+  gemm<true, false>(s, H, H, B, v.dH2, H, v.A1, H, gW2, H, 0);
+  colsum_kernel<<<blocks_for(H), 256, 0, s>>>(B, H, v.dH2, gb2);
+  gemm<false, false>(s, B, H, H, v.dH2, H, v.W2, H, v.dH1, H, 0);
+  gelu_back_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>((long long)B * H, v.dH1, v.Z1);
+  gemm<true, false>(s, H, nin, B, v.dH1, H, x, nin, gW1, nin, 0);
+  colsum_kernel<<<blocks_for(H), 256, 0, s>>>(B, H, v.dH1, gb1);
+  return mlp_status();
+}
+
+int nexd_mlp_adam(int64_t count, float* params, const float* grads, float* m, float* v, int32_t step, float lr,
+                  float beta1, float beta2, float eps, void* stream) {
+  if (count < 1 || !params || !grads || !m || !v || step < 1) return set_err(nullptr, NEXD_ERR_INVALID, "bad Adam arguments");
+  const float c1 = 1.f - std::pow(beta1, float(step)), c2 = 1.f - std::pow(beta2, float(step));
+  adam_kernel<<<blocks_for(count), 256, 0, static_cast<cudaStream_t>(stream)>>>(count, params, grads, m, v, lr, beta1,
+                                                                                   beta2, eps, c1, c2);
+  return mlp_status();
 }
 
 }  // extern "C"

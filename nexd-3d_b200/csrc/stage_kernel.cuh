@@ -137,7 +137,36 @@ struct StageArgs {
   int last_stage;
   const int* pml_off;    // [nbatch] 1 once the STA/LTA trigger switched the NPML off
   int* flag;             // error bits: 1 non-finite trace (record kernel), 2 tensor-core wait timed out
+  const float* ghost;    // learned boundary: [nbatch][nbf][9][NpF] exterior states (face code -3 - index)
+  int nbf;
 };
+
+// Jump q+ - q- at one face node for a face code: neighbour trace (>= 0),
+// free surface (-1: own trace, flagged), absorbing (-2: exterior state zero)
+// or learned absorbing (<= -3: exterior state from the ghost buffer).
+template <int NpF>
+__device__ __forceinline__ bool face_jump(const StageArgs& a, int b, int code, int fi, const float* tr, const float* qo,
+                                          int qs, float* dq) {
+  if (code >= 0) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dq[c] = tr[c] - qo[c * qs];
+    return false;
+  }
+  if (code == -1) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dq[c] = qo[c * qs];
+    return true;
+  }
+  if (code == -2) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dq[c] = -qo[c * qs];
+    return false;
+  }
+  const float* gh = a.ghost + ((long long)b * a.nbf + (-3 - code)) * 9 * NpF + fi;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) dq[c] = gh[c * NpF] - qo[c * qs];
+  return false;
+}
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 
@@ -605,19 +634,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       const int own = sPat[f * NpF + fi];  // patterns 0..3 are the element's own face masks
       const float* qo = sQF + ee * Np + own;
       float dq[9];
-      bool free_face = false;
-      if (code >= 0) {
-        const float* tr = sTr + i * 9;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = tr[c] - qo[c * (E * Np)];
-      } else if (code == -1) {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = qo[c * (E * Np)];
-        free_face = true;
-      } else {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = -qo[c * (E * Np)];
-      }
+      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, E * Np, dq);
       float ap, as1, as2;
       face_amplitudes(g, f, dq, free_face, ap, as1, as2);
       const float fs = g[G_FS + f];

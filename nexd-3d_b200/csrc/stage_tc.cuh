@@ -208,19 +208,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
       const int own = sPat[f * NpF + fi];
       const float* qo = sQF + ee * Np + own;
       float dq[9];
-      bool free_face = false;
-      if (code >= 0) {
-        const float* tr = sTr + i * 9;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = tr[c] - qo[c * (E * Np)];
-      } else if (code == -1) {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = qo[c * (E * Np)];
-        free_face = true;
-      } else {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) dq[c] = -qo[c * (E * Np)];
-      }
+      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, E * Np, dq);
       float ap, as1, as2;
       face_amplitudes(g, f, dq, free_face, ap, as1, as2);
       const float fs = g[G_FS + f];

@@ -63,10 +63,12 @@ HOST_SYMBOLS = ["nexd_mesh_build", "nexd_mesh_desc", "nexd_mesh_get_info", "nexd
                 "nexd_mesh_last_error", "nexd_mesh_free"]
 GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
                "nexd_get_state", "nexd_set_state", "nexd_step_io", "nexd_pml_trigger", "nexd_get_energy",
-               "nexd_set_contraction", "nexd_get_contraction",
+               "nexd_set_contraction", "nexd_get_contraction", "nexd_boundary_faces", "nexd_set_boundary_mlp",
+               "nexd_get_ghost", "nexd_get_face_traces", "nexd_mlp_param_count", "nexd_mlp_workspace_floats",
+               "nexd_mlp_forward", "nexd_mlp_loss_grad", "nexd_mlp_adam",
                "nexd_wavefield_energy_noalloc", "nexd_profile_enable", "nexd_profile_get",
                "nexd_last_error", "nexd_launch_count", "nexd_destroy"]
-NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_ENERGY, NEXD_K_COUNT = 0, 1, 2, 3, 4
+NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_ENERGY, NEXD_K_BOUNDARY, NEXD_K_COUNT = 0, 1, 2, 3, 4, 5
 
 
 class NexdProfile(C.Structure):
@@ -125,6 +127,19 @@ def gpu_lib():
         lib.nexd_get_energy.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.nexd_set_contraction.argtypes = [vp, C.c_int32]
         lib.nexd_get_contraction.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
+        i32p = C.POINTER(C.c_int32)
+        lib.nexd_boundary_faces.argtypes = [vp, i32p, i32p, i32p]
+        lib.nexd_set_boundary_mlp.argtypes = [vp, C.POINTER(C.c_float), C.c_int64, C.c_float]
+        lib.nexd_get_ghost.argtypes = [vp, C.POINTER(C.c_float)]
+        lib.nexd_get_face_traces.argtypes = [vp, C.c_int32, i32p, i32p, C.POINTER(C.c_float)]
+        lib.nexd_mlp_param_count.argtypes = [C.c_int32, C.c_int32]
+        lib.nexd_mlp_param_count.restype = C.c_int64
+        lib.nexd_mlp_workspace_floats.argtypes = [C.c_int32, C.c_int32, C.c_int32]
+        lib.nexd_mlp_workspace_floats.restype = C.c_int64
+        lib.nexd_mlp_forward.argtypes = [C.c_int32, C.c_int32, vp, vp, C.c_int32, vp, vp, vp]
+        lib.nexd_mlp_loss_grad.argtypes = [C.c_int32, C.c_int32, vp, vp, vp, C.c_int32, vp, vp, vp, vp]
+        lib.nexd_mlp_adam.argtypes = [C.c_int64, vp, vp, vp, vp, C.c_int32, C.c_float, C.c_float, C.c_float,
+                                      C.c_float, vp]
         lib.nexd_wavefield_energy_noalloc.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32,
                                                       C.POINTER(C.c_double)]
         lib.nexd_profile_enable.argtypes = [vp, C.c_int32]

@@ -84,7 +84,7 @@ class Solver:
             return None
         p = _abi.NexdProfile()
         lib.nexd_profile_get(self._ctx, C.byref(p))
-        names = ("record", "stage_pml", "stage_main", "energy")
+        names = ("record", "stage_pml", "stage_main", "energy", "boundary")
         out = {n: dict(launches=p.launches[i], ms=p.ms[i], elements=p.elements[i]) for i, n in enumerate(names)}
         out["span_ms"] = p.span_ms
         return out
@@ -109,6 +109,56 @@ class Solver:
         names = {0: "fp32", 1: "bf16x3"}
         return ({"npml": names[kinds[0]], "rest": names[kinds[1]]},
                 {(cl, names[k]): ms[2 * i + k] for i, cl in enumerate(("npml", "rest")) for k in range(2)})
+
+    def boundary_faces(self):
+        """(elem, face) 1-based arrays of the absorbing faces in ghost-slot order."""
+        lib = _abi.gpu_lib()
+        n = C.c_int32()
+        st = lib.nexd_boundary_faces(self._ctx, C.byref(n), None, None)
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+        e = np.zeros(n.value, dtype=np.int32)
+        f = np.zeros(n.value, dtype=np.int32)
+        if n.value:
+            st = lib.nexd_boundary_faces(self._ctx, None, e.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         f.ctypes.data_as(C.POINTER(C.c_int32)))
+            if st != 0:
+                raise _gpu_error(self._ctx, st)
+        return e, f
+
+    def set_boundary_mlp(self, params, max_reflection=0.5):
+        """Learned absorbing boundary from FP32 parameters (incoming characteristics
+        bounded by max_reflection times the outgoing ones), or None for the plain one."""
+        lib = _abi.gpu_lib()
+        if params is None:
+            st = lib.nexd_set_boundary_mlp(self._ctx, None, 0, 0.0)
+        else:
+            p = np.ascontiguousarray(params, dtype=np.float32)
+            st = lib.nexd_set_boundary_mlp(self._ctx, p.ctypes.data_as(C.POINTER(C.c_float)), p.size,
+                                           max_reflection)
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+
+    def ghost(self, npf):
+        """Exterior states of the last stage, (nbatch, nbf, 9, NpF)."""
+        nbf = len(self.boundary_faces()[0])
+        out = np.zeros((self.nbatch, nbf, 9, npf), dtype=np.float32)
+        st = _abi.gpu_lib().nexd_get_ghost(self._ctx, out.ctypes.data_as(C.POINTER(C.c_float)))
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+        return out
+
+    def face_traces(self, elem, face, npf):
+        """Own and neighbour traces of faces (1-based elem, face): (nbatch, nfaces, 2, 9, NpF)."""
+        e = np.ascontiguousarray(elem, dtype=np.int32)
+        f = np.ascontiguousarray(face, dtype=np.int32)
+        out = np.zeros((self.nbatch, len(e), 2, 9, npf), dtype=np.float32)
+        st = _abi.gpu_lib().nexd_get_face_traces(self._ctx, len(e), e.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 f.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 out.ctypes.data_as(C.POINTER(C.c_float)))
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+        return out
 
     def pml_trigger(self, avg_window1=10, avg_window2=2, sta_lta_trigger=0.1, f0=1.0, formula=0):
         """Arm the NPML energy STA/LTA trigger (src/timeloopMod.f90:508-542)."""

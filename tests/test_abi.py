@@ -13,7 +13,7 @@ from nexd_b200 import _abi, Mesh, synth
 
 def _declared(header):
     txt = open(os.path.join(ROOT, "include", header)).read()
-    return sorted(set(re.findall(r"^(?:int|const nexd_desc\*|void)\s+(nexd_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^(?:int|int64_t|const nexd_desc\*|void)\s+(nexd_\w+)\s*\(", txt, re.M)))
 
 
 def _exported(lib):

@@ -1,0 +1,187 @@
+"""Learned absorbing boundary on the GPU, through the C-ABI: the MLP training
+kernels against the FP64 oracle (oracle/mlp_oracle.py), the ghost-state kernel
+against the same network evaluated on the host, the zero-output network
+against the plain absorbing boundary, and a trained network against the plain
+boundary on a held-out source, both judged by the wide-NPML run.
+
+Tolerances: gradients and outputs of the FP32 training kernels within 1e-4
+relative L2 of FP64; the ghost kernel (BF16 weights, FP32 accumulation)
+within 1e-4 of the host evaluation with the same BF16 weights.
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from nexd_b200 import Mesh, boundary, synth
+from nexd_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import mlp_oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+NIN, H = 135, 128
+
+
+@pytest.fixture(scope="module")
+def Solver():
+    from nexd_b200.solver import Solver as S
+    return S
+
+
+def _random_params(rng, scale_out=0.3):
+    p = boundary.init_params(NIN, H, seed=int(rng.integers(1 << 30)))
+    W1, b1, W2, b2, W3, b3 = mlp_oracle.unpack(p, NIN, H)
+    rest = np.concatenate([W1.ravel(), rng.standard_normal(H) * 0.1, W2.ravel(), rng.standard_normal(H) * 0.1,
+                           rng.standard_normal(NIN * H) * scale_out / np.sqrt(H), rng.standard_normal(NIN) * 0.05])
+    return rest.astype(np.float32)
+
+
+def test_mlp_kernels_match_oracle():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(3)
+    B = 96
+    p = _random_params(rng)
+    x = rng.standard_normal((B, NIN)).astype(np.float32)
+    t = rng.standard_normal((B, NIN)).astype(np.float32)
+    tr = boundary.Trainer(NIN, params=p, batch=B)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    tr.loss_grad(xd, td)
+    torch.cuda.synchronize()
+    loss_ref, g_ref = mlp_oracle.loss_grad(p, x, t, NIN, H)
+    assert abs(float(tr.loss[0]) - loss_ref) / loss_ref < 1e-5
+    g = tr.grads.cpu().numpy().astype(np.float64)
+    assert rel_l2(g, g_ref) < 1e-4
+    # every parameter block has its gradient
+    o = 0
+    for n in (H * NIN, H, H * H, H, NIN * H, NIN):
+        assert rel_l2(g[o:o + n], g_ref[o:o + n]) < 1e-4
+        o += n
+    # forward
+    y = torch.zeros((B, NIN), dtype=torch.float32, device="cuda")
+    lib = _abi.gpu_lib()
+    assert lib.nexd_mlp_forward(NIN, H, tr._ptr(tr.params), tr._ptr(xd), B, tr._ptr(y), tr._ptr(tr.work), None) == 0
+    y_ref, _ = mlp_oracle.forward(p.astype(np.float64), x.astype(np.float64), NIN, H)
+    assert rel_l2(y.cpu().numpy(), y_ref) < 1e-5
+    # one Adam step: p - lr * m_hat / (sqrt(v_hat) + eps) with m = (1-b1) g, v = (1-b2) g^2
+    g32 = tr.grads.clone()
+    assert lib.nexd_mlp_adam(tr.count, tr._ptr(tr.params), tr._ptr(g32), tr._ptr(tr.m), tr._ptr(tr.v), 1,
+                             1e-3, 0.9, 0.999, 1e-8, None) == 0
+    gg = g32.cpu().numpy().astype(np.float64)
+    p1 = p - 1e-3 * gg / (np.abs(gg) + 1e-8)
+    assert np.allclose(tr.params.cpu().numpy(), p1, rtol=1e-5, atol=1e-7)
+
+
+def _absorbing_cube(tmp_path, nt=20):
+    d = str(tmp_path / "cube")
+    synth.write_cube(d, cells=4, nt=nt)
+    return Mesh(d, N=4, stf_stage_time=True)
+
+
+def test_zero_output_network_is_the_plain_boundary(tmp_path, Solver):
+    """W3 = 0, b3 = 0: every ghost state is zero, so the run is bit-identical
+    to the plain absorbing boundary."""
+    m = _absorbing_cube(tmp_path)
+    a, b = Solver(m.desc_ptr), Solver(m.desc_ptr)
+    b.set_boundary_mlp(boundary.init_params(NIN, H, seed=1), max_reflection=0.9)
+    a.run(1, 20)
+    b.run(1, 20)
+    assert np.array_equal(a.field(), b.field())
+    assert np.array_equal(a.traces(), b.traces())
+    assert b.profile() is not None
+    assert np.all(b.ghost(m.NpF) == 0.0)
+    b.set_boundary_mlp(None)  # back to the plain boundary
+    b.run(1, 20)
+
+
+def test_ghost_kernel_matches_host_network(tmp_path, Solver):
+    """One Euler stage from a random wavefield: the device ghost states equal
+    the host evaluation (features -> RMS -> network with the same BF16
+    weights -> states)."""
+    d = str(tmp_path / "cube")
+    synth.write_cube(d, cells=4, nt=2)
+    m = Mesh(d, N=4, timeint=1)
+    rng = np.random.default_rng(5)
+    s = Solver(m.desc_ptr)
+    q0 = np.asfortranarray((rng.standard_normal((m.K * m.Np, 9)) * np.array([1e6] * 6 + [0.1] * 3)).astype(np.float32))
+    s.set_field(q0)
+    p = _random_params(rng)
+    s.set_boundary_mlp(p, max_reflection=0.7)
+    e, f = s.boundary_faces()
+    own = s.face_traces(e, f, m.NpF)[0][:, 0].astype(np.float64)  # (nbf, 9, NpF) before the step
+    s.run(1, 1)
+    ghost = s.ghost(m.NpF)[0]
+    n, s_, t, zp, zs = boundary.face_frames(m, e, f)
+    x = boundary.features(own, n, s_, t, zp, zs)
+    xn, _, r = boundary.normalise(x)
+    y, _ = mlp_oracle.forward(torch_free_bf16(p), xn, NIN, H)
+    ref = boundary.ghost_states(xn, y, r, n, s_, t, zp, 0.7, m.NpF)
+    assert np.abs(ref).max() > 0
+    assert rel_l2(ghost, ref) < 1e-4
+
+
+def torch_free_bf16(p):
+    """FP32 -> BF16 (round to nearest even) -> FP64."""
+    u = np.asarray(p, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def test_face_traces_match_state(tmp_path, Solver):
+    """Own traces are the element's face nodes; neighbour traces of interior
+    faces are the neighbour's matching nodes (same coordinates)."""
+    m = _absorbing_cube(tmp_path, nt=2)
+    s = Solver(m.desc_ptr)
+    rng = np.random.default_rng(2)
+    q0 = np.asfortranarray(rng.standard_normal((m.K * m.Np, 9)).astype(np.float32))
+    s.set_field(q0)
+    fm = m.array("fmask")
+    nb, fc = m.array("neighbor"), m.array("face")
+    x, y, zc = m.array("vx"), m.array("vy"), m.array("vz")
+    elems = np.arange(1, m.K + 1, 7, dtype=np.int32)
+    faces = (np.arange(len(elems)) % 4 + 1).astype(np.int32)
+    tr = s.face_traces(elems, faces, m.NpF)[0]
+    for i, (e, f) in enumerate(zip(elems - 1, faces - 1)):
+        nodes = e * m.Np + fm[:, f] - 1
+        assert np.array_equal(tr[i, 0], q0[nodes].T)
+        if fc[f, e] > 0:
+            en = nb[f, e] - 1
+            other = tr[i, 1]
+            # each neighbour trace value sits at a neighbour node with the same coordinates
+            for k in range(m.NpF):
+                j = nodes[k]
+                cand = en * m.Np + np.arange(m.Np)
+                hit = cand[np.argmin((x[cand] - x[j]) ** 2 + (y[cand] - y[j]) ** 2 + (zc[cand] - zc[j]) ** 2)]
+                assert np.array_equal(other[:, k], q0[hit])
+        else:
+            assert np.all(tr[i, 1] == 0)
+
+
+def test_learned_boundary_beats_plain_boundary(tmp_path, Solver):
+    """Train on wide-NPML runs of the method (five seeded sources, 8-element
+    NPML around a 2 x 2 x 1 km two-layer model), evaluate on a held-out
+    source: against the wide run, the learned boundary's velocity-field error
+    inside the small model once the waves have reached its boundary, and its
+    surface velocity-trace misfit, are below the plain absorbing boundary's."""
+    pytest.importorskip("torch")
+    cells, h, P, dur = (8, 8, 4), 250.0, 8, 1.2
+    srcs = boundary.random_sources(6, cells, h, seed=11)
+    pairs = [boundary.ModelPair(str(tmp_path), f"s{i}", src, cells=cells, h=h, pml_cells=P, duration=dur)
+             for i, src in enumerate(srcs)]
+    xs, ys = zip(*(p.training_pairs(Solver, every=2) for p in pairs[:5]))
+    x, y = np.concatenate(xs), np.concatenate(ys)
+    tr = boundary.Trainer(NIN, batch=2048, lr=1e-3, seed=0)
+    base = tr.evaluate(x, y)
+    hist = tr.fit(x, y, epochs=30)
+    assert hist[-1] < 0.5 * base, (base, hist)
+    ev = pairs[5]
+    cps = [int(ev.nt * 0.6), int(ev.nt * 0.8), ev.nt]
+    res = ev.evaluate(Solver, tr.parameters(), cps, max_reflection=0.3)
+    plain, learned = res["plain"], res["learned"]
+    print("plain", plain, "learned", learned)
+    assert np.mean(learned["field_err"]) < 0.95 * np.mean(plain["field_err"])
+    assert learned["trace_err"] < plain["trace_err"]
