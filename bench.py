@@ -46,7 +46,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "nexd-3d_b200")
 sys.path.insert(0, PKG)
 
-from nexd_b200 import Mesh, synth, _abi  # noqa: E402
+from nexd_b200 import Mesh, synth, _abi, replicas  # noqa: E402
 
 WORKLOADS = {
     "twolayer": dict(name="twolayer_anelastic_npml_192k_tets_N4_lserk4", cells=(40, 40, 20), N=4, nt=3000),
@@ -58,42 +58,6 @@ N_ORDER = 4
 # CPU sample: same model family and order at 20x20x10 cells (24,000 tets)
 CPU_SAMPLE_CELLS = (20, 20, 10)
 CPU_SAMPLE_STEPS = 6
-
-
-def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    if ws <= 1:
-        return 0, 1, 0, None
-    import torch
-    import torch.distributed as dist
-    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    from datetime import timedelta
-    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-    return rank, ws, local, dist
-
-
-def barrier(dist):
-    if dist is not None:
-        dist.barrier()
-
-
-def max_over_ranks(dist, x):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def sum_over_ranks(dist, x):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
 
 
 def load_peaks():
@@ -187,7 +151,8 @@ def main():
     ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
     ap.add_argument("--cells", default=None, help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
     args = ap.parse_args()
-    rank, world, local, dist = dist_init()
+    grp = replicas.init()
+    rank, world, local = grp.rank, grp.world, grp.local
     wl = WORKLOADS[args.workload]
     cells = wl["cells"] if args.cells is None else tuple(int(x) for x in args.cells.split(","))
     workload = wl["name"] if cells == wl["cells"] else \
@@ -210,16 +175,17 @@ def main():
             return
         from nexd_b200.solver import Solver
         import torch
-        if dist is None:
+        if grp.dist is None:
             torch.cuda.set_device(0)
         d = os.path.join(tmp, "model")
         if args.workload == "cube":
-            synth.write_cube(d, cells=cells[0], nt=wl["nt"], seed=1 + rank)
+            synth.write_cube(d, cells=cells[0], nt=wl["nt"], seed=replicas.replica_seed(1, rank))
             mesh = Mesh(d, N=wl["N"], stf_stage_time=True)
         else:
             nsrc = wl.get("nsrc", 1)
             kw = dict(src_depth=(500.0, 1800.0), f0_range=(2.0, 4.0)) if nsrc > 1 else {}
-            synth.write_twolayer(d, cells=cells, nt=wl["nt"], nrec=100, nsrc=nsrc, src_seed=2 + rank, **kw)
+            synth.write_twolayer(d, cells=cells, nt=wl["nt"], nrec=100, nsrc=nsrc,
+                                 src_seed=replicas.replica_seed(2, rank), **kw)
             mesh = Mesh(d, N=wl["N"], stf_stage_time=True, nbatch=nsrc)
         s = Solver(mesh.desc_ptr)
         s.set_contraction(args.contraction)
@@ -228,7 +194,7 @@ def main():
         if need > mesh.nt:
             raise SystemExit(f"--warmup + 3*--steps must be <= {mesh.nt}")
         s.run(1, warmup)
-        barrier(dist)
+        grp.barrier()
         torch.cuda.synchronize()
         clk_file = os.path.join(tmp, "clocks.csv")
         clk = sample_clocks(None, clk_file) if rank == 0 else None
@@ -236,7 +202,7 @@ def main():
         # timed region: K steps, CUDA graphs, run-span events only
         l0 = s.launch_count()
         s.profile("span")
-        barrier(dist)
+        grp.barrier()
         torch.cuda.synchronize()
         s.run(warmup + 1, warmup + steps)
         torch.cuda.synchronize()
@@ -251,22 +217,22 @@ def main():
         if clk:
             clk.terminate()
             clk.wait()
-        dev_ms = max_over_ranks(dist, span["span_ms"])
+        dev_ms = grp.max(span["span_ms"])
         units = 9 * mesh.Np * mesh.K * nstage * steps * mesh.nbatch
-        total_units = sum_over_ranks(dist, units)
+        total_units = grp.sum(units)
         value = total_units / (dev_ms * 1e-3)
         # end to end through the streaming C-ABI call, host buffers in and out
         nspt, nsrc, nrec = mesh.desc.stf_per_step, mesh.nsrc, mesh.nrec
         stf_all = mesh.array("stf")  # (nspt, nt, nsrc)
         stf_in = np.zeros((nspt, nsrc), dtype=np.float32, order="F")
         tr_out = np.zeros((nrec, 9, mesh.nbatch), dtype=np.float32, order="F")
-        barrier(dist)
+        grp.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for it in range(warmup + 2 * steps + 1, warmup + 3 * steps + 1):
             stf_in[:, :] = stf_all[:, it - 1, :]
             s.step_io(it, stf_in, tr_out)
-        e2e_s = max_over_ranks(dist, time.perf_counter() - t0)
+        e2e_s = grp.max(time.perf_counter() - t0)
         e2e = total_units / e2e_s
         if rank != 0:
             return
@@ -318,8 +284,7 @@ def main():
         s.close()
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
-        if dist is not None:
-            dist.destroy_process_group()
+        grp.close()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,66 @@
+"""The multi-GPU path of bench.py on CPU: two gloo ranks run the replica
+plumbing (torchrun environment, barrier, max/sum reductions, whole-job
+throughput, per-rank seeded sources) that bench.py runs over NCCL."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import PKG
+
+torch = pytest.importorskip("torch")
+import torch.multiprocessing as mp  # noqa: E402
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out_dir):
+    sys.path.insert(0, PKG)
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    from nexd_b200 import replicas, synth
+    g = replicas.init("gloo", timeout_s=60)
+    assert (g.rank, g.world) == (rank, world)
+    g.barrier()
+    seconds = 1.0 + rank          # rank 1 is the slow one
+    units = 100.0 * (rank + 1)
+    res = dict(max=g.max(seconds), sum=g.sum(units), agg=replicas.aggregate(g, units, seconds))
+    d = os.path.join(out_dir, f"r{rank}")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=5, nrec=2, src_seed=replicas.replica_seed(2, rank))
+    src = open(os.path.join(d, "data", "source")).read()
+    g.barrier()
+    g.close()
+    np.save(os.path.join(out_dir, f"res{rank}.npy"), np.array([res["max"], res["sum"], res["agg"]]))
+    with open(os.path.join(out_dir, f"src{rank}.txt"), "w") as f:
+        f.write(src)
+
+
+def test_two_gloo_ranks(tmp_path):
+    world, port = 2, _free_port()
+    mp.start_processes(_rank_main, args=(world, port, str(tmp_path)), nprocs=world, join=True, start_method="spawn")
+    r0, r1 = (np.load(tmp_path / f"res{r}.npy") for r in range(world))
+    # max of the times, sum of the units, whole-job throughput = sum / max
+    assert np.allclose(r0, r1)
+    assert r0[0] == 2.0 and r0[1] == 300.0 and np.isclose(r0[2], 150.0)
+    # each rank's replica has its own seeded source
+    assert open(tmp_path / "src0.txt").read() != open(tmp_path / "src1.txt").read()
+
+
+def test_single_process_group_is_local():
+    sys.path.insert(0, PKG)
+    from nexd_b200 import replicas
+    env = {k: os.environ.pop(k) for k in ("WORLD_SIZE", "RANK") if k in os.environ}
+    try:
+        g = replicas.init()
+        assert g.dist is None and g.world == 1
+        assert g.max(3.0) == 3.0 and g.sum(5.0) == 5.0 and replicas.aggregate(g, 10.0, 2.0) == 5.0
+        g.barrier()
+        g.close()
+    finally:
+        os.environ.update(env)
