@@ -53,7 +53,97 @@ WORKLOADS = {
     "cube": dict(name="cube_elastic_absorbing_6k_tets_N3_lserk4", cells=(10, 10, 10), N=3, nt=1000),
     "batch64": dict(name="twolayer_anelastic_npml_192k_tets_N4_lserk4_64_sources", cells=(40, 40, 20), N=4,
                     nt=2000, nsrc=64),
+    "multimodel": dict(name="16_models_8k_to_300k_tets_N2_to_5_one_graph", cells=None, N=None, nt=1500),
 }
+
+
+def multimodel_specs(seed=4, n=16):
+    """16 seeded models: sizes 8,000-300,000 tets (log-uniform), orders 2-5,
+    elastic or 3-mechanism anelastic, homogeneous or two-layer, absorbing
+    sides and bottom, one double-couple source and 25 surface receivers each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        k = float(np.exp(rng.uniform(np.log(8000.0), np.log(300000.0))))
+        nz = max(2, int(round((k / 24.0) ** (1.0 / 3.0))))
+        out.append(dict(cells=(2 * nz, 2 * nz, nz), N=int(rng.choice([2, 3, 4, 5])), att=bool(rng.random() < 0.5),
+                        homogeneous=bool(rng.random() < 0.5), src_seed=int(rng.integers(1 << 30))))
+    return out
+
+
+def run_multimodel(args, grp, tmp, steps, warmup):
+    """Config 4: the 16 models stepped together as one CUDA graph, grids autotuned."""
+    from nexd_b200.solver import Solver, Group
+    import torch
+    torch.cuda.set_device(0 if grp.dist is None else grp.local)
+    meshes, solvers = [], []
+    for i, sp in enumerate(multimodel_specs(seed=replicas.replica_seed(4, grp.rank))):
+        d = os.path.join(tmp, f"model{i}")
+        synth.write_twolayer(d, cells=sp["cells"], nt=WORKLOADS["multimodel"]["nt"], nrec=25, nsrc=1,
+                             attenuation=sp["att"], pml=False, src_depth=(500.0, 500.0), src_seed=sp["src_seed"],
+                             homogeneous=sp["homogeneous"])
+        m = Mesh(d, N=sp["N"], stf_stage_time=True)
+        s = Solver(m.desc_ptr)
+        meshes.append(m)
+        solvers.append(s)
+    g = Group(solvers)
+    div = g.autotune()
+    g.run(1, warmup)
+    grp.barrier()
+    torch.cuda.synchronize()
+    clk_file = os.path.join(tmp, "clocks.csv")
+    clk = sample_clocks(None, clk_file) if grp.rank == 0 else None
+    time.sleep(0.3 if clk else 0)
+    l0 = sum(s.launch_count() for s in solvers)
+    g.run(warmup + 1, warmup + steps)
+    span_ms = g.span_ms()
+    launches = sum(s.launch_count() for s in solvers) - l0
+    # end to end: K more steps from the host call to the traces of every model in host memory
+    t0 = time.perf_counter()
+    g.run(warmup + steps + 1, warmup + 2 * steps)
+    trace_bytes = 0
+    for s in solvers:
+        trace_bytes += s.traces().nbytes
+    e2e_s = grp.max(time.perf_counter() - t0)
+    if clk:
+        clk.terminate()
+        clk.wait()
+    units = sum(9 * m.Np * m.K * 5 * steps for m in meshes)
+    total = grp.sum(units)
+    dev_ms = grp.max(span_ms)
+    value = total / (dev_ms * 1e-3)
+    abytes = sum(algorithmic_bytes(m, "stage_main", m.K) for m in meshes) * 5 * steps
+    achieved = grp.sum(abytes) / (dev_ms * 1e-3) / 1e9
+    peak, peak_kind = load_peaks()
+    if grp.rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline and grp.world == 1:
+        v, cores, sample = oracle_baseline(tmp, "twolayer")
+        cpu = {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
+    line = {
+        "metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": grp.world, "steps": steps,
+        "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (16 seeded models per rank)",
+        "config": {"workload": WORKLOADS["multimodel"]["name"],
+                   "models": [dict(tets=m.K, N=m.N, anelastic=bool(m.desc.attenuation)) for m in meshes],
+                   "total_tets": int(sum(m.K for m in meshes)), "integrator": "LSERK4 (5 stages)",
+                   "timed": "one CUDA graph per two steps, one branch per model; grids autotuned",
+                   "grid_divisor": div, "l2": "inputs larger than L2",
+                   "parallelism": f"replicas x{grp.world}"},
+        "roofline": {"bound": "hbm", "kernel": "all stage kernels of the group (step average)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_kind},
+        "e2e": {"value": total / e2e_s, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(trace_bytes / steps)},
+        "gpu_launches": int(launches),
+        "cpu_baseline": cpu,
+        "clocks": summarize_clocks(clk_file, grp.local) if clk else None,
+    }
+    print(json.dumps(line), flush=True)
+    g.close()
+    for s in solvers:
+        s.close()
 N_ORDER = 4
 # CPU sample: same model family and order at 20x20x10 cells (24,000 tets)
 CPU_SAMPLE_CELLS = (20, 20, 10)
@@ -157,6 +247,15 @@ def main():
     cells = wl["cells"] if args.cells is None else tuple(int(x) for x in args.cells.split(","))
     workload = wl["name"] if cells == wl["cells"] else \
         wl["name"].replace("192k_tets", f"{6 * cells[0] * cells[1] * cells[2]}_tets")
+    if args.workload == "multimodel" and args.impl == "ours":
+        steps, warmup = args.steps, max(3, args.warmup)
+        tmp = tempfile.mkdtemp(prefix=f"nexd_bench_{rank}_")
+        try:
+            run_multimodel(args, grp, tmp, steps, warmup)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+            grp.close()
+        return
     steps, warmup = args.steps, max(3, args.warmup)
     tmp = tempfile.mkdtemp(prefix=f"nexd_bench_{rank}_")
     metric = "DOF-stage updates/s"

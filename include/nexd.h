@@ -305,6 +305,24 @@ int nexd_mlp_loss_grad(int32_t n_in, int32_t n_hidden, const float* params, cons
 int nexd_mlp_adam(int64_t count, float* params, const float* grads, float* m, float* v, int32_t step, float lr,
                   float beta1, float beta2, float eps, void* stream);
 
+/* ---- Several models in one CUDA graph (no counterpart in the reference) ------
+ * A group replays the steps of its member contexts (any orders, sizes,
+ * rheologies and contractions) as one CUDA graph with one concurrent branch
+ * per member on the member's stream, captured for two steps and replayed;
+ * members keep their own state, step counter and traces, and a group run is
+ * bit-identical to running the members one by one.  nexd_group_run runs steps
+ * it_begin..it_end of every member (within every member's nt).
+ * nexd_group_autotune times harmless first-stage launches of all members
+ * running together (they leave the live state unchanged) with the members'
+ * persistent grids divided by 1, 2 or 4 and keeps the fastest divisor.
+ * nexd_group_span: device time of the last nexd_group_run (CUDA events). */
+typedef struct nexd_group nexd_group;
+int nexd_group_create(nexd_ctx* const* members, int32_t n, nexd_group** out);
+int nexd_group_run(nexd_group* group, int32_t it_begin, int32_t it_end);
+int nexd_group_autotune(nexd_group* group, int32_t* divisor);
+int nexd_group_span(const nexd_group* group, double* span_ms);
+int nexd_group_destroy(nexd_group* group);
+
 /* Timing of nexd_run with CUDA events on the library's stream, counters reset:
  * on = 0 off; 1 per-launch events per kernel kind plus the run span (steps are
  * launched one kernel at a time); 2 run span only (steps replay captured

@@ -100,6 +100,7 @@ struct nexd_ctx {
   bool use_graphs = true;
   // element contraction: NEXD_CONTRACT_FP32 (CUDA cores) or NEXD_CONTRACT_BF16X3 (tensor cores)
   int contraction = NEXD_CONTRACT_FP32;
+  int grid_div = 1;            // persistent grid divided by this (models sharing the GPU in a group)
   int kind[2] = {NEXD_CONTRACT_FP32, NEXD_CONTRACT_FP32};  // kernel per element class: [0] NPML, [1] the rest
   float tune_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};           // autotune: [class][kind] ms per launch
   uint4* ops_tc = nullptr;     // packed operator of the tensor-core kernels (order 4)
@@ -356,7 +357,7 @@ int configure_launch(nexd_ctx* c) {
     const int nel = pmlk ? c->Kpml : c->K - c->Kpml;
     const int E = elements_per_chunk(c->N);
     const long long work = (long long)((nel + E - 1) / E) * c->nbatch;
-    const int grid = int(std::max<long long>(1, std::min<long long>(work, (long long)per_sm * c->nsm)));
+    const int grid = int(std::max<long long>(1, std::min<long long>(work, (long long)per_sm * c->nsm / c->grid_div)));
     if (pmlk) { c->grid_pml = grid; c->smem_pml = smem; }
     else { c->grid_main = grid; c->smem_main = smem; }
   }
@@ -1411,6 +1412,217 @@ int nexd_mlp_adam(int64_t count, float* params, const float* grads, float* m, fl
   adam_kernel<<<blocks_for(count), 256, 0, static_cast<cudaStream_t>(stream)>>>(count, params, grads, m, v, lr, beta1,
                                                                                    beta2, eps, c1, c2);
   return mlp_status();
+}
+
+// ---- several models in one CUDA graph --------------------------------------------
+
+}  // extern "C"
+
+struct nexd_group {
+  std::vector<nexd_ctx*> m;
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, span[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<int> parity;       // members' buffer parity when the graph was captured
+  std::vector<int> graph_launches;
+  float span_ms = 0.f;
+  std::string err;
+};
+
+namespace {
+
+int gerr(nexd_group* g, int code, const std::string& msg) {
+  if (g) g->err = msg;
+  return set_err(nullptr, code, msg);
+}
+
+#define GCUDA(g, call)                                                                         \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return gerr(g, NEXD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+void drop_group_graph(nexd_group* g) {
+  if (g->gexec) {
+    cudaGraphExecDestroy(g->gexec);
+    g->gexec = nullptr;
+  }
+}
+
+// Members' work forked from the group stream and joined back: `body` enqueues
+// one member's work on the member's stream.
+template <class F>
+int fork_join(nexd_group* g, F body) {
+  GCUDA(g, cudaEventRecord(g->fork, g->s));
+  for (size_t i = 0; i < g->m.size(); ++i) {
+    nexd_ctx* c = g->m[i];
+    GCUDA(g, cudaStreamWaitEvent(c->stream, g->fork, 0));
+    body(i, c);
+    GCUDA(g, cudaEventRecord(g->join[i], c->stream));
+    GCUDA(g, cudaStreamWaitEvent(g->s, g->join[i], 0));
+  }
+  return NEXD_OK;
+}
+
+int capture_group(nexd_group* g) {
+  drop_group_graph(g);
+  cudaGraph_t graph = nullptr;
+  GCUDA(g, cudaStreamBeginCapture(g->s, cudaStreamCaptureModeThreadLocal));
+  std::vector<int64_t> before(g->m.size());
+  int st = fork_join(g, [&](size_t i, nexd_ctx* c) {
+    before[i] = c->launches;
+    enqueue_body(c, 2);
+  });
+  cudaError_t e = cudaStreamEndCapture(g->s, &graph);
+  for (size_t i = 0; i < g->m.size(); ++i) {
+    g->graph_launches[i] = int(g->m[i]->launches - before[i]);
+    g->m[i]->launches = before[i];
+    g->parity[i] = g->m[i]->cur;
+  }
+  if (st) return st;
+  if (e != cudaSuccess) return gerr(g, NEXD_ERR_CUDA, std::string("group capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&g->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return gerr(g, NEXD_ERR_CUDA, std::string("group instantiate: ") + cudaGetErrorString(e));
+  return NEXD_OK;
+}
+
+// Harmless first-stage launches of every member (as in the contraction autotune).
+void enqueue_probe(nexd_ctx* c, int reps) {
+  StageArgs a = base_args(c);
+  a.stage = 0;
+  a.stage_first = 1;
+  a.last_stage = 0;
+  a.ca = c->timeint == 4 ? 0.f : 1.f;
+  a.cb = 0.f;
+  a.q_in = c->qbuf[c->cur];
+  a.q_out = c->qbuf[(c->cur + 1) % (c->timeint == 3 ? 3 : 2)];
+  a.q_n = c->qbuf[c->cur];
+  set_step_kernel<<<1, 32, 0, c->stream>>>(c->it_dev, 1);
+  for (int r = 0; r < reps; ++r) {
+    if (c->Kpml > 0) launch_class(c, a, true);
+    if (c->K > c->Kpml) launch_class(c, a, false);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int nexd_group_create(nexd_ctx* const* members, int32_t n, nexd_group** out) {
+  if (!out || !members || n < 1) return set_err(nullptr, NEXD_ERR_INVALID, "bad group arguments");
+  *out = nullptr;
+  auto* g = new nexd_group();
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) {
+      delete g;
+      return set_err(nullptr, NEXD_ERR_INVALID, "null member");
+    }
+    for (nexd_ctx* o : g->m)
+      if (o == members[i]) {
+        delete g;
+        return set_err(nullptr, NEXD_ERR_INVALID, "a context appears twice in the group");
+      }
+    g->m.push_back(members[i]);
+  }
+  g->join.assign(n, nullptr);
+  g->parity.assign(n, -1);
+  g->graph_launches.assign(n, 0);
+  cudaError_t e = cudaStreamCreateWithFlags(&g->s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&g->join[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreate(&g->span[0]);
+  if (e == cudaSuccess) e = cudaEventCreate(&g->span[1]);
+  if (e != cudaSuccess) {
+    nexd_group_destroy(g);
+    return set_err(nullptr, NEXD_ERR_CUDA, std::string("group set-up: ") + cudaGetErrorString(e));
+  }
+  *out = g;
+  return NEXD_OK;
+}
+
+int nexd_group_run(nexd_group* g, int32_t it_begin, int32_t it_end) {
+  if (!g) return set_err(nullptr, NEXD_ERR_INVALID, "null group");
+  for (nexd_ctx* c : g->m) {
+    if (it_begin < 1 || it_end > c->nt || it_begin > it_end)
+      return gerr(g, NEXD_ERR_INVALID, "step range out of 1..nt of a member");
+    if (c->profiling) return gerr(g, NEXD_ERR_INVALID, "per-launch timing is on in a member");
+  }
+  GCUDA(g, cudaEventRecord(g->span[0], g->s));
+  for (nexd_ctx* c : g->m) set_step_kernel<<<1, 32, 0, g->s>>>(c->it_dev, it_begin);
+  int n = it_end - it_begin + 1;
+  if (n >= 2) {
+    bool stale = !g->gexec;
+    for (size_t i = 0; i < g->m.size(); ++i) stale |= g->parity[i] != g->m[i]->cur;
+    if (stale)
+      if (int st = capture_group(g)) return st;
+    for (; n >= 2; n -= 2) {
+      GCUDA(g, cudaGraphLaunch(g->gexec, g->s));
+      for (size_t i = 0; i < g->m.size(); ++i) g->m[i]->launches += g->graph_launches[i];
+    }
+  }
+  if (n == 1)
+    if (int st = fork_join(g, [&](size_t, nexd_ctx* c) { enqueue_body(c, 1); })) return st;
+  GCUDA(g, cudaEventRecord(g->span[1], g->s));
+  GCUDA(g, cudaEventSynchronize(g->span[1]));
+  GCUDA(g, cudaEventElapsedTime(&g->span_ms, g->span[0], g->span[1]));
+  for (nexd_ctx* c : g->m)
+    if (int st = finish(c)) return gerr(g, st, c->err);
+  return NEXD_OK;
+}
+
+int nexd_group_autotune(nexd_group* g, int32_t* divisor) {
+  if (!g) return set_err(nullptr, NEXD_ERR_INVALID, "null group");
+  const int cand[3] = {1, 2, 4};
+  float best_ms = 0.f;
+  int best = 1;
+  for (int k = 0; k < 3; ++k) {
+    for (nexd_ctx* c : g->m) {
+      c->grid_div = cand[k];
+      if (int st = configure_launch(c)) return gerr(g, st, c->err);
+    }
+    if (int st = fork_join(g, [&](size_t, nexd_ctx* c) { enqueue_probe(c, 1); })) return st;  // warm-up
+    GCUDA(g, cudaEventRecord(g->span[0], g->s));
+    if (int st = fork_join(g, [&](size_t, nexd_ctx* c) { enqueue_probe(c, 3); })) return st;
+    GCUDA(g, cudaEventRecord(g->span[1], g->s));
+    GCUDA(g, cudaEventSynchronize(g->span[1]));
+    GCUDA(g, cudaGetLastError());
+    float ms = 0.f;
+    GCUDA(g, cudaEventElapsedTime(&ms, g->span[0], g->span[1]));
+    if (k == 0 || ms < best_ms) {
+      best_ms = ms;
+      best = cand[k];
+    }
+  }
+  for (nexd_ctx* c : g->m) {
+    c->grid_div = best;
+    if (int st = configure_launch(c)) return gerr(g, st, c->err);
+    drop_graphs(c);
+  }
+  drop_group_graph(g);
+  if (divisor) *divisor = best;
+  return NEXD_OK;
+}
+
+int nexd_group_span(const nexd_group* g, double* span_ms) {
+  if (!g || !span_ms) return set_err(nullptr, NEXD_ERR_INVALID, "null argument");
+  *span_ms = g->span_ms;
+  return NEXD_OK;
+}
+
+int nexd_group_destroy(nexd_group* g) {
+  if (!g) return NEXD_OK;
+  if (g->s) cudaStreamSynchronize(g->s);
+  drop_group_graph(g);
+  if (g->fork) cudaEventDestroy(g->fork);
+  for (cudaEvent_t e : g->join)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : g->span)
+    if (e) cudaEventDestroy(e);
+  if (g->s) cudaStreamDestroy(g->s);
+  delete g;
+  return NEXD_OK;
 }
 
 }  // extern "C"

@@ -191,3 +191,47 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+class Group:
+    """Several solvers stepped together as one CUDA graph (nexd_group_*)."""
+
+    def __init__(self, solvers):
+        lib = _abi.gpu_lib()
+        self._members = list(solvers)  # keeps the contexts alive
+        arr = (C.c_void_p * len(self._members))(*[s._ctx.value for s in self._members])
+        g = C.c_void_p()
+        st = lib.nexd_group_create(arr, len(self._members), C.byref(g))
+        if st != 0:
+            raise _gpu_error(None, st)
+        self._g = g
+
+    def run(self, it_begin, it_end):
+        st = _abi.gpu_lib().nexd_group_run(self._g, it_begin, it_end)
+        if st != 0:
+            raise _gpu_error(None, st)
+
+    def autotune(self):
+        d = C.c_int32()
+        st = _abi.gpu_lib().nexd_group_autotune(self._g, C.byref(d))
+        if st != 0:
+            raise _gpu_error(None, st)
+        return d.value
+
+    def span_ms(self):
+        v = C.c_double()
+        st = _abi.gpu_lib().nexd_group_span(self._g, C.byref(v))
+        if st != 0:
+            raise _gpu_error(None, st)
+        return v.value
+
+    def close(self):
+        if getattr(self, "_g", None):
+            _abi.gpu_lib().nexd_group_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -190,11 +190,12 @@ def write_cube(directory, *, cells=10, seed=1, nt=1000):
 
 
 def write_twolayer(directory, *, cells=(40, 40, 20), seed=2, nt=3000, nrec=100, nsrc=1, attenuation=True,
-                   pml=True, f0=3.0, src_depth=(1500.0, 1500.0), f0_range=None, src_seed=None):
+                   pml=True, f0=3.0, src_depth=(1500.0, 1500.0), f0_range=None, src_seed=None, homogeneous=False):
     """Two-layer anelastic box 4x4x2 km (40x40x20 hexahedra x 6 = 192,000 tets):
     upper 600 m vp 3000 / vs 1730 / rho 2400 / Qp 100 / Qs 50, half-space 5000 /
     2890 / 2800 / 400 / 200; 3-cell NPML on the sides and bottom, free top;
-    seeded double-couple sources (Ricker), random surface receivers."""
+    seeded double-couple sources (Ricker), random surface receivers.
+    homogeneous: the half-space material everywhere."""
     Lx, Ly, Lz = 4000.0, 4000.0, 2000.0
     nx, ny, nz = cells
     rng = np.random.default_rng(seed if src_seed is None else src_seed)
@@ -217,6 +218,7 @@ def write_twolayer(directory, *, cells=(40, 40, 20), seed=2, nt=3000, nrec=100, 
     if pml:
         par.update(set_pml=".true.", pml_delta=3 * hx, pml_rc=0.001, pml_kmax=1.0, pml_afac=1.0)
     return write_simulation(directory, box=(0, Lx, 0, Ly, 0, Lz), cells=cells, jitter=0.05, seed=seed,
-                            layers=[(Lz - 600.0, 3000.0, 1730.0, 2400.0, 100.0, 50.0),
-                                    (-math.inf, 5000.0, 2890.0, 2800.0, 400.0, 200.0)],
+                            layers=([(-math.inf, 5000.0, 2890.0, 2800.0, 400.0, 200.0)] if homogeneous else
+                                    [(Lz - 600.0, 3000.0, 1730.0, 2400.0, 100.0, 50.0),
+                                     (-math.inf, 5000.0, 2890.0, 2800.0, 400.0, 200.0)]),
                             pml_cells=3 if pml else 0, parfile=par, sources=srcs, stations=recs)

@@ -1,0 +1,84 @@
+"""Several models in one CUDA graph (nexd_group_*): a group run is
+bit-identical to running its members one by one, for members of different
+orders, sizes, rheologies and contractions, over step pairs and a leftover
+step; the grid autotune leaves the live state unchanged."""
+import numpy as np
+import pytest
+
+from nexd_b200 import Mesh, synth
+from nexd_b200 import _abi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def solver_mod():
+    from nexd_b200 import solver
+    return solver
+
+
+def _models(tmp_path):
+    out = []
+    d = str(tmp_path / "cube2")
+    synth.write_cube(d, cells=4, nt=30)
+    out.append((Mesh(d, N=2, stf_stage_time=True), "fp32"))
+    d = str(tmp_path / "tl3")
+    synth.write_twolayer(d, cells=(8, 8, 4), nt=30, nrec=4, src_depth=(900.0, 900.0))
+    out.append((Mesh(d, N=3, stf_stage_time=True), "fp32"))
+    d = str(tmp_path / "tl4")
+    synth.write_twolayer(d, cells=(8, 8, 4), nt=30, nrec=4, src_depth=(900.0, 900.0), attenuation=False,
+                         src_seed=7)
+    out.append((Mesh(d, N=4, stf_stage_time=True), "bf16x3"))
+    return out
+
+
+def test_group_run_equals_member_runs(tmp_path, solver_mod):
+    models = _models(tmp_path)
+    alone = []
+    for m, c in models:
+        s = solver_mod.Solver(m.desc_ptr)
+        s.set_contraction(c)
+        s.run(1, 13)
+        alone.append((s.field(), s.traces()))
+    members = []
+    for m, c in models:
+        s = solver_mod.Solver(m.desc_ptr)
+        s.set_contraction(c)
+        members.append(s)
+    g = solver_mod.Group(members)
+    g.run(1, 6)       # three graph replays
+    g.run(7, 13)      # three replays and a leftover step
+    assert g.span_ms() > 0
+    for s, (f, t) in zip(members, alone):
+        assert np.array_equal(s.field(), f)
+        assert np.array_equal(s.traces(), t)
+    g.close()
+
+
+def test_group_autotune_keeps_state(tmp_path, solver_mod):
+    models = _models(tmp_path)
+    members = [solver_mod.Solver(m.desc_ptr) for m, _ in models]
+    g = solver_mod.Group(members)
+    g.run(1, 4)
+    before = [s.field() for s in members]
+    div = g.autotune()
+    assert div in (1, 2, 4)
+    for s, f in zip(members, before):
+        assert np.array_equal(s.field(), f)
+    g.run(5, 8)
+    ref = [solver_mod.Solver(m.desc_ptr) for m, _ in models]
+    for r in ref:
+        r.run(1, 8)
+    for s, r in zip(members, ref):
+        assert np.array_equal(s.field(), r.field())
+
+
+def test_group_errors(tmp_path, solver_mod):
+    models = _models(tmp_path)
+    a = solver_mod.Solver(models[0][0].desc_ptr)
+    with pytest.raises(Exception):
+        solver_mod.Group([a, a])
+    g = solver_mod.Group([a])
+    with pytest.raises(Exception):
+        g.run(1, 31)  # beyond nt
+    g.run(1, 2)
