@@ -96,3 +96,18 @@ def test_oracle_header_is_test_infrastructure():
         p = os.path.join(PKG, "lib", lib)
         if os.path.exists(p):
             assert not any(s.startswith("oracle_") for s in _exported(p))
+
+
+def test_fortran_module_binds_declared_entry_points():
+    """nexd-3d_b200/fortran/nexd_capi.f90 (the Fortran host's ISO_C_BINDING
+    module) binds only names the header declares, and its nexd_desc lists the
+    C struct's fields in the same order."""
+    src = open(os.path.join(PKG, "fortran", "nexd_capi.f90")).read()
+    bound = set(re.findall(r'bind\(C, name="(nexd_\w+)"\)', src))
+    assert bound and bound <= set(_declared("nexd.h"))
+    body = src[src.index("type, bind(C) :: nexd_desc"):src.index("end type nexd_desc")]
+    names = []
+    for line in body.splitlines()[1:]:
+        if "::" in line:
+            names += [n.strip() for n in line.split("::")[1].split(",")]
+    assert names == [f[0] for f in _abi.NexdDesc._fields_]
