@@ -256,6 +256,17 @@ int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
  * (0 where not measured).  Either pointer may be NULL. */
 int nexd_get_contraction(const nexd_ctx* ctx, int32_t* kinds, float* tune_ms);
 
+/* ---- Movie snapshots (src/timeloopMod.f90:482-489, 576-581; collectMovieMod.f90) ----
+ * With frame > 0 every step integrates the displacement u += dt v at every
+ * node on the device (from the start value, 1e-24 in the reference) and every
+ * frame-th step stores the per-element mean of |u| over the element's nodes
+ * (the cell value collectMovie writes to movie_elem_it*.vtk) for up to
+ * max_frames frames; frame = 0 switches it off. */
+int nexd_movie(nexd_ctx* ctx, int32_t frame, int32_t max_frames);
+/* Stored frames: *nframes; out (NULL to query) (nelem, nframes, nbatch) in the
+ * mesh's element order. */
+int nexd_get_movie(nexd_ctx* ctx, float* out, int32_t* nframes);
+
 /* ---- Learned absorbing boundary (no counterpart in the reference) ----------
  * Absorbing faces (face code -2) normally take the exterior state as zero
  * (computeExactRiemannSF with -VT, src/waveMod.f90:269-336).  The upwind flux

@@ -115,6 +115,11 @@ struct nexd_ctx {
   float mlp_rho = 0.f;               // bound of the incoming / outgoing characteristic ratio
   int ghost_grid = 0;
   size_t ghost_smem = 0;
+  // movie: nodal displacement and per-element frames (src/timeloopMod.f90:482-489, 576-581)
+  int movie_frame = 0, movie_max = 0, movie_last_it = 0;
+  float init_value = 0.f;            // start value of every field (the reference's 1e-24)
+  float* movie_u = nullptr;          // [nbatch][3][ldq]
+  float* movie_buf = nullptr;        // [max_frames][nbatch][K] (internal element order)
   int* gather_idx = nullptr;         // face-trace gather scratch
   float* gather_out = nullptr;
   int gather_cap = 0;
@@ -598,6 +603,7 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   for (int i = 0; i < nq; ++i) {
     if ((st = dalloc(c, &c->qbuf[i], size_t(nb) * 9 * c->ldq))) return fail(st);
     if ((st = fill(c, c->qbuf[i], size_t(nb) * 9 * c->ldq, float(d->init_value)))) return fail(st);
+    c->init_value = float(d->init_value);
   }
   if (c->timeint == 4) {
     if ((st = dalloc(c, &c->res, size_t(nb) * 9 * c->ldq))) return fail(st);
@@ -724,6 +730,40 @@ void ev_collect(nexd_ctx* c) {
     }
   }
   c->ev_used = 0;
+}
+
+// u += dt v at every node (after the step, as src/timeloopMod.f90:482-485) and,
+// every `frame`-th step, the element mean of |u| (collectMovieMod.f90's cell
+// value) into frame slot it/frame - 1.  Block: 256 threads = E elements x Np nodes.
+__global__ void movie_kernel(const float* q, float* u, long long ldq, int K, int Np, int nbatch, float dt,
+                             const int* it_dev, int frame, int max_frames, float* frames) {
+  __shared__ float red[256];
+  const int E = 256 / Np;
+  const int le = threadIdx.x / Np, n = threadIdx.x - le * Np;
+  const int b = blockIdx.y;
+  const int e = blockIdx.x * E + le;
+  float mag = 0.f;
+  if (le < E && e < K) {
+    const long long node = (long long)e * Np + n;
+    const float* qb = q + (long long)b * 9 * ldq;
+    float* ub = u + (long long)b * 3 * ldq;
+    float s2 = 0.f;
+    for (int c = 0; c < 3; ++c) {
+      const float v = ub[c * ldq + node] + dt * qb[(6 + c) * ldq + node];
+      ub[c * ldq + node] = v;
+      s2 += v * v;
+    }
+    mag = sqrtf(s2);
+  }
+  red[threadIdx.x] = mag;
+  __syncthreads();
+  const int it = *it_dev;
+  if (it % frame != 0 || it / frame > max_frames) return;
+  if (le < E && n == 0 && e < K) {
+    float sum = 0.f;
+    for (int k = 0; k < Np; ++k) sum += red[le * Np + k];
+    frames[((long long)(it / frame - 1) * nbatch + b) * K + e] = sum / Np;
+  }
 }
 
 __global__ void set_step_kernel(int* it_dev, int it) {
@@ -917,6 +957,13 @@ void enqueue_body(nexd_ctx* c, int nsteps) {
       ev_end(c, ev);
       c->launches += 2;
     }
+    if (c->movie_frame > 0) {
+      const int E = 256 / c->Np;
+      movie_kernel<<<dim3((c->K + E - 1) / E, c->nbatch), 256, 0, c->stream>>>(
+          c->qbuf[c->cur], c->movie_u, c->ldq, c->K, c->Np, c->nbatch, float(c->dt), c->it_dev, c->movie_frame,
+          c->movie_max, c->movie_buf);
+      ++c->launches;
+    }
     tick_kernel<<<1, 32, 0, c->stream>>>(c->it_dev);
     ++c->launches;
   }
@@ -934,6 +981,7 @@ void drop_graphs(nexd_ctx* c) {
 // graph (the ping-pong parity returns to its start after two steps for every
 // integrator), a leftover single step and profiled runs launch directly.
 int enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
+  c->movie_last_it = std::max(c->movie_last_it, it_end);
   set_step_kernel<<<1, 32, 0, c->stream>>>(c->it_dev, it_begin);
   int n = it_end - it_begin + 1;
   if (c->profiling || !c->use_graphs || n < 2) {
@@ -1166,6 +1214,46 @@ int nexd_get_energy(nexd_ctx* c, double* energy, int32_t* pml_switch) {
   if (pml_switch)
     CUDA_TRY(c, cudaMemcpyAsync(pml_switch, c->pml_switch, c->nbatch * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return NEXD_OK;
+}
+
+// ---- movie snapshots ---------------------------------------------------------
+
+int nexd_movie(nexd_ctx* c, int32_t frame, int32_t max_frames) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (frame < 0 || (frame > 0 && max_frames < 1)) return set_err(c, NEXD_ERR_INVALID, "bad movie arguments");
+  drop_graphs(c);
+  if (frame == 0) {
+    c->movie_frame = 0;
+    return NEXD_OK;
+  }
+  int st;
+  if (!c->movie_u) {
+    const size_t n = size_t(c->nbatch) * 3 * c->ldq;
+    if ((st = dalloc(c, &c->movie_u, n)) || (st = fill(c, c->movie_u, n, c->init_value))) return st;
+  }
+  if (max_frames > c->movie_max) {
+    if ((st = dalloc(c, &c->movie_buf, size_t(max_frames) * c->nbatch * c->K))) return st;
+    CUDA_TRY(c, cudaMemset(c->movie_buf, 0, size_t(max_frames) * c->nbatch * c->K * sizeof(float)));
+    c->movie_max = max_frames;
+  }
+  c->movie_frame = frame;
+  return NEXD_OK;
+}
+
+int nexd_get_movie(nexd_ctx* c, float* out, int32_t* nframes) {
+  if (!c || !nframes) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  if (c->movie_frame <= 0 || !c->movie_buf) {
+    *nframes = 0;
+    return NEXD_OK;
+  }
+  const int nf = std::min(c->movie_max, c->movie_last_it / c->movie_frame);
+  *nframes = nf;
+  if (!out || nf == 0) return NEXD_OK;
+  std::vector<float> h(size_t(nf) * c->nbatch * c->K);
+  CUDA_TRY(c, cudaMemcpy(h.data(), c->movie_buf, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  for (size_t fb = 0; fb < size_t(nf) * c->nbatch; ++fb)
+    for (int ni = 0; ni < c->K; ++ni) out[fb * c->K + c->new2old[ni]] = h[fb * c->K + ni];
   return NEXD_OK;
 }
 
@@ -1550,7 +1638,10 @@ int nexd_group_run(nexd_group* g, int32_t it_begin, int32_t it_end) {
     if (c->profiling) return gerr(g, NEXD_ERR_INVALID, "per-launch timing is on in a member");
   }
   GCUDA(g, cudaEventRecord(g->span[0], g->s));
-  for (nexd_ctx* c : g->m) set_step_kernel<<<1, 32, 0, g->s>>>(c->it_dev, it_begin);
+  for (nexd_ctx* c : g->m) {
+    set_step_kernel<<<1, 32, 0, g->s>>>(c->it_dev, it_begin);
+    c->movie_last_it = std::max(c->movie_last_it, it_end);
+  }
   int n = it_end - it_begin + 1;
   if (n >= 2) {
     bool stale = !g->gexec;

@@ -160,6 +160,26 @@ class Solver:
             raise _gpu_error(self._ctx, st)
         return out
 
+    def movie(self, frame, max_frames=64):
+        """Per-element |u| snapshots every `frame` steps (0 switches them off)."""
+        st = _abi.gpu_lib().nexd_movie(self._ctx, frame, max_frames)
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+
+    def movie_frames(self):
+        """Stored snapshots, (nbatch, nframes, nelem)."""
+        lib = _abi.gpu_lib()
+        nf = C.c_int32()
+        st = lib.nexd_get_movie(self._ctx, None, C.byref(nf))
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+        out = np.zeros((self.nbatch, nf.value, self.K), dtype=np.float32)
+        if nf.value:
+            st = lib.nexd_get_movie(self._ctx, out.ctypes.data_as(C.POINTER(C.c_float)), C.byref(nf))
+            if st != 0:
+                raise _gpu_error(self._ctx, st)
+        return out
+
     def pml_trigger(self, avg_window1=10, avg_window2=2, sta_lta_trigger=0.1, f0=1.0, formula=0):
         """Arm the NPML energy STA/LTA trigger (src/timeloopMod.f90:508-542)."""
         st = _abi.gpu_lib().nexd_pml_trigger(self._ctx, avg_window1, avg_window2, sta_lta_trigger, f0, formula)

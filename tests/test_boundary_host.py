@@ -94,3 +94,26 @@ def test_mlp_oracle_gradient_matches_finite_differences():
         dp[i] = eps
         fd = (mlp_oracle.loss_grad(p + dp, x, t, nin, h)[0] - mlp_oracle.loss_grad(p - dp, x, t, nin, h)[0]) / (2 * eps)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])
+
+
+def test_vtk_cell_scalars_format(tmp_path):
+    """movie_elem_it*.vtk in the layout of the reference's
+    writeVtkTetraMeshRealdata (legacy ASCII, CELLS of 4 corners, type 10,
+    CELL_DATA 'data')."""
+    from nexd_b200 import synth, vtk
+    d = str(tmp_path / "m")
+    synth.write_cube(d, cells=2, nt=2)
+    coord, tets = vtk.read_cubit_mesh(d)
+    data = np.arange(len(tets), dtype=float) * 0.5
+    p = vtk.write_movie(d, str(tmp_path / "out"), [data], frame_step=10)[0]
+    assert p.endswith("movie_elem_it0000010.vtk")
+    lines = open(p).read().split("\n")
+    assert lines[:4] == ["# vtk DataFile Version 3.1", "Mesh with Data", "ASCII", "DATASET UNSTRUCTURED_GRID"]
+    assert lines[4].split() == ["POINTS", str(len(coord)), "float"]
+    i = lines.index(next(l for l in lines if l.startswith("CELLS")))
+    assert lines[i].split()[1:] == [str(len(tets)), str(5 * len(tets))]
+    cells = np.array([l.split() for l in lines[i + 1:i + 1 + len(tets)]], dtype=int)
+    assert (cells[:, 0] == 4).all() and np.array_equal(cells[:, 1:], tets)
+    j = lines.index(next(l for l in lines if l.startswith("CELL_DATA")))
+    assert lines[j + 1] == "SCALARS data float" and lines[j + 2] == "LOOKUP_TABLE default"
+    assert np.allclose(np.array(lines[j + 3:j + 3 + len(tets)], dtype=float), data)
