@@ -66,7 +66,7 @@ WORKLOADS = {
 }
 
 
-def train_learned_boundary(tmp, n_train=8, n_eval=4, seed=11):
+def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.5):
     """Config 5 at training scale: a 2 x 2 x 1 km two-layer model (1,536 tets)
     inside an 8-element NPML; train the boundary MLP on n_train sources,
     score plain and learned boundaries against the wide run on n_eval
@@ -87,12 +87,12 @@ def train_learned_boundary(tmp, n_train=8, n_eval=4, seed=11):
     params = tr.parameters()
     scores = []
     for ev in pairs[n_train:]:
-        res = ev.evaluate(Solver, params, [int(ev.nt * 0.6), int(ev.nt * 0.8), ev.nt], max_reflection=0.3)
+        res = ev.evaluate(Solver, params, [int(ev.nt * 0.6), int(ev.nt * 0.8), ev.nt], max_reflection=max_reflection)
         scores.append(res)
     mean = lambda k, f: float(np.mean([np.mean(r[k][f]) for r in scores]))
     summary = {"train_sources": n_train, "heldout_sources": n_eval, "samples": int(len(x)),
                "loss_first_last": [hist[0], hist[-1]], "data_s": round(t_data, 1), "train_s": round(t_train, 1),
-               "max_reflection": 0.3,
+               "max_reflection": max_reflection,
                "field_err_vs_wide_npml": {"plain": mean("plain", "field_err"), "learned": mean("learned", "field_err")},
                "trace_err_vs_wide_npml": {"plain": mean("plain", "trace_err"), "learned": mean("learned", "trace_err")},
                "judge": "8-element NPML around the model (the method itself)"}
