@@ -393,7 +393,8 @@ def main():
         tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
         if os.path.exists(tp):
             try:
-                t = json.load(open(tp)).get(workload, {}).get(dom)
+                kind = s.contraction()[0]["npml" if dom == "stage_pml" else "rest"]
+                t = json.load(open(tp)).get(workload, {}).get(f"{dom}/{kind}")
                 traffic = None if t is None else float(t)
             except Exception:
                 traffic = None
