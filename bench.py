@@ -277,7 +277,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--contraction", default="fp32", choices=["fp32", "bf16x3", "auto"],
+    ap.add_argument("--contraction", default="auto", choices=["fp32", "bf16x3", "auto"],
                     help="element contraction: FP32 CUDA cores, split-BF16 tcgen05 tensor cores, or the faster "
                          "per element class (timed before the run)")
     ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
@@ -332,7 +332,7 @@ def main():
                                  src_seed=replicas.replica_seed(2, rank), pml=(args.workload != "learned"), **kw)
             mesh = Mesh(d, N=wl["N"], stf_stage_time=True, nbatch=nsrc)
         s = Solver(mesh.desc_ptr)
-        s.set_contraction(args.contraction)
+        s.set_contraction(args.contraction if mesh.N == 4 else "fp32")  # the tensor-core kernels cover N=4
         if learned is not None:
             s.set_boundary_mlp(lb_params, learned["max_reflection"])
         nstage = 5
@@ -407,9 +407,13 @@ def main():
         line = {
             "metric": metric, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded two-layer model, per-rank seeded source)",
+            "vs_baseline": None,
+            "dtype": "f32" if set(s.contraction()[0].values()) == {"fp32"} else
+                     "f32 state and update; contraction as three-way split bf16 on tcgen05 with f32 accumulation",
+            "data": "synthetic (seeded two-layer model, per-rank seeded source)",
             "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
-                       "integrator": "LSERK4 (5 stages)", "contraction": args.contraction,
+                       "integrator": "LSERK4 (5 stages)",
+                       "contraction": args.contraction if mesh.N == 4 else "fp32",
                        "kernels_per_class": s.contraction()[0], "pml_tets": int(prof["stage_pml"]["elements"]),
                        "receivers": nrec, "sources_per_rank": nsrc, "wavefields_per_rank": nb,
                        "timed": "CUDA graphs of two steps; roofline from a per-launch-event pass of K more steps",
