@@ -126,6 +126,7 @@ def run_multimodel(args, grp, tmp, steps, warmup):
                              homogeneous=sp["homogeneous"])
         m = Mesh(d, N=sp["N"], stf_stage_time=True)
         s = Solver(m.desc_ptr)
+        s.set_contraction(args.contraction if (m.N == 4 or args.contraction != "bf16x3") else "fp32")
         meshes.append(m)
         solvers.append(s)
     g = Group(solvers)
@@ -168,7 +169,8 @@ def run_multimodel(args, grp, tmp, steps, warmup):
         "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (16 seeded models per rank)",
         "config": {"workload": WORKLOADS["multimodel"]["name"],
-                   "models": [dict(tets=m.K, N=m.N, anelastic=bool(m.desc.attenuation)) for m in meshes],
+                   "models": [dict(tets=m.K, N=m.N, anelastic=bool(m.desc.attenuation),
+                                   kernel=s.contraction()[0]["rest"]) for m, s in zip(meshes, solvers)],
                    "total_tets": int(sum(m.K for m in meshes)), "integrator": "LSERK4 (5 stages)",
                    "timed": "one CUDA graph per two steps, one branch per model; grids autotuned",
                    "grid_divisor": div, "l2": "inputs larger than L2",
@@ -277,7 +279,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--contraction", default="auto", choices=["fp32", "bf16x3", "auto"],
+    ap.add_argument("--contraction", default="auto", choices=["fp32", "bf16x3", "auto", "fp32_pairs"],
                     help="element contraction: FP32 CUDA cores, split-BF16 tcgen05 tensor cores, or the faster "
                          "per element class (timed before the run)")
     ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
@@ -332,7 +334,8 @@ def main():
                                  src_seed=replicas.replica_seed(2, rank), pml=(args.workload != "learned"), **kw)
             mesh = Mesh(d, N=wl["N"], stf_stage_time=True, nbatch=nsrc)
         s = Solver(mesh.desc_ptr)
-        s.set_contraction(args.contraction if mesh.N == 4 else "fp32")  # the tensor-core kernels cover N=4
+        contraction = args.contraction if (mesh.N == 4 or args.contraction != "bf16x3") else "fp32"
+        s.set_contraction(contraction)  # the tensor-core kernels cover N=4
         if learned is not None:
             s.set_boundary_mlp(lb_params, learned["max_reflection"])
         nstage = 5
@@ -413,7 +416,7 @@ def main():
             "data": "synthetic (seeded two-layer model, per-rank seeded source)",
             "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
                        "integrator": "LSERK4 (5 stages)",
-                       "contraction": args.contraction if mesh.N == 4 else "fp32",
+                       "contraction": contraction,
                        "kernels_per_class": s.contraction()[0], "pml_tets": int(prof["stage_pml"]["elements"]),
                        "receivers": nrec, "sources_per_rank": nsrc, "wavefields_per_rank": nb,
                        "timed": "CUDA graphs of two steps; roofline from a per-launch-event pass of K more steps",

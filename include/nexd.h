@@ -243,17 +243,25 @@ typedef struct nexd_profile {
  * (NEXD_ERR_UNSUPPORTED otherwise).  The state, the stage update and
  * everything else stay FP32.  No counterpart in the reference (its loop is
  * FP32 matvecs).
- * NEXD_CONTRACT_AUTO times both kernels on this mesh (a few stage launches
- * at the current step boundary that leave the live state unchanged) and keeps
- * the faster one per element class (NPML elements, the rest); results of the
- * two agree to FP32 rounding, not bit for bit. */
-enum nexd_contraction { NEXD_CONTRACT_FP32 = 0, NEXD_CONTRACT_BF16X3 = 1, NEXD_CONTRACT_AUTO = 2 };
+ * NEXD_CONTRACT_AUTO times the candidate kernels on this mesh (a few stage
+ * launches at the current step boundary that leave the live state unchanged)
+ * and keeps the fastest per element class (NPML elements, the rest): the FP32
+ * kernel, the tensor-core kernel (order 4) and, outside the NPML, an FP32
+ * kernel with a thread per node pair (orders 2-5; bit-identical to the FP32
+ * kernel).  Results of the FP32 and tensor-core kernels agree to FP32
+ * rounding, not bit for bit.  NEXD_CONTRACT_AUTO is accepted for every order. */
+enum nexd_contraction {
+  NEXD_CONTRACT_FP32 = 0,
+  NEXD_CONTRACT_BF16X3 = 1,
+  NEXD_CONTRACT_AUTO = 2,
+  NEXD_CONTRACT_FP32_PAIRS = 3  /* FP32; the node-pair kernel outside the NPML (orders 2-5) */
+};
 int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
 
 /* The kernel kind in use per element class (kinds[0] NPML elements, kinds[1]
- * the rest: NEXD_CONTRACT_FP32 or NEXD_CONTRACT_BF16X3) and, after an AUTO
- * selection, the measured ms per stage launch tune_ms[class * 2 + kind]
- * (0 where not measured).  Either pointer may be NULL. */
+ * the rest: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3 or 2 = the node-pair FP32
+ * kernel) and, after an AUTO selection, the measured ms per stage launch
+ * tune_ms[class * 3 + kind] (0 where not measured).  Either pointer may be NULL. */
 int nexd_get_contraction(const nexd_ctx* ctx, int32_t* kinds, float* tune_ms);
 
 /* ---- Movie snapshots (src/timeloopMod.f90:482-489, 576-581; collectMovieMod.f90) ----

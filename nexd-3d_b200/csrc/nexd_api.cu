@@ -18,6 +18,7 @@
 #include "energy_kernel.cuh"
 #include "stage_kernel.cuh"
 #include "stage_tc.cuh"
+#include "stage_pair.cuh"
 #include "boundary_mlp.cuh"
 
 using namespace nexd_dev;
@@ -102,7 +103,7 @@ struct nexd_ctx {
   int contraction = NEXD_CONTRACT_FP32;
   int grid_div = 1;            // persistent grid divided by this (models sharing the GPU in a group)
   int kind[2] = {NEXD_CONTRACT_FP32, NEXD_CONTRACT_FP32};  // kernel per element class: [0] NPML, [1] the rest
-  float tune_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};           // autotune: [class][kind] ms per launch
+  float tune_ms[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}; // autotune: [class][kind] ms per launch
   uint4* ops_tc = nullptr;     // packed operator of the tensor-core kernels (order 4)
   // learned absorbing boundary: absorbing faces, their ghost states and the MLP
   int nbf = 0;                       // absorbing faces
@@ -283,6 +284,29 @@ std::vector<uint16_t> pack_tc_operator(const nexd_desc* d) {
   return out;
 }
 
+template <int N>
+KernelFn pick_pair(bool att, int mode) {
+  if (mode == MODE_LSERK) return att ? stage_pair_kernel<N, true, MODE_LSERK> : stage_pair_kernel<N, false, MODE_LSERK>;
+  return att ? stage_pair_kernel<N, true, MODE_TVD> : stage_pair_kernel<N, false, MODE_TVD>;
+}
+
+// The node-pair FP32 kernel (elements outside the NPML; orders 2-5).
+KernelFn pick_pair_kernel(int N, bool att, int mode, size_t& smem) {
+  switch (N) {
+    case 2: smem = size_t(Order<2, 2>::smem_floats(false)) * 4; return pick_pair<2>(att, mode);
+    case 3: smem = size_t(Order<3, 2>::smem_floats(false)) * 4; return pick_pair<3>(att, mode);
+    case 4: smem = size_t(Order<4, 2>::smem_floats(false)) * 4; return pick_pair<4>(att, mode);
+    case 5: smem = size_t(Order<5, 2>::smem_floats(false)) * 4; return pick_pair<5>(att, mode);
+    default: smem = 0; return nullptr;
+  }
+}
+
+// Kernel kinds per element class: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3
+// and the node-pair FP32 kernel (same results as NEXD_CONTRACT_FP32, chosen
+// by the autotune only).
+constexpr int KIND_FP32_PAIRS = 2;
+constexpr int NKINDS = 3;
+
 int elements_per_chunk(int N) {
   const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
   return 256 / Np;
@@ -352,15 +376,21 @@ int configure_launch(nexd_ctx* c) {
     const bool pmlk = which == 0;
     size_t smem = 0;
     const void* fn;
-    if (c->kind[which] == NEXD_CONTRACT_BF16X3) fn = reinterpret_cast<const void*>(pick_tc_kernel(c->N, c->att, pmlk, mode, smem));
-    else fn = reinterpret_cast<const void*>(pick_kernel(c->N, c->att, pmlk, mode, smem));
+    int E = elements_per_chunk(c->N);
+    if (c->kind[which] == NEXD_CONTRACT_BF16X3) {
+      fn = reinterpret_cast<const void*>(pick_tc_kernel(c->N, c->att, pmlk, mode, smem));
+    } else if (c->kind[which] == KIND_FP32_PAIRS && !pmlk) {
+      fn = reinterpret_cast<const void*>(pick_pair_kernel(c->N, c->att, mode, smem));
+      E *= 2;
+    } else {
+      fn = reinterpret_cast<const void*>(pick_kernel(c->N, c->att, pmlk, mode, smem));
+    }
     if (!fn) return set_err(c, NEXD_ERR_UNSUPPORTED, "no stage kernel for this order and contraction");
     CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
     CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
     if (per_sm < 1) return set_err(c, NEXD_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
     const int nel = pmlk ? c->Kpml : c->K - c->Kpml;
-    const int E = elements_per_chunk(c->N);
     const long long work = (long long)((nel + E - 1) / E) * c->nbatch;
     const int grid = int(std::max<long long>(1, std::min<long long>(work, (long long)per_sm * c->nsm / c->grid_div)));
     if (pmlk) { c->grid_pml = grid; c->smem_pml = smem; }
@@ -785,6 +815,9 @@ void launch_class(nexd_ctx* c, StageArgs& a, bool pml) {
   if (c->kind[cls] == NEXD_CONTRACT_BF16X3) {
     TcKernelFn f = pick_tc_kernel(c->N, c->att, pml, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a, c->ops_tc);
+  } else if (c->kind[cls] == KIND_FP32_PAIRS && !pml) {
+    KernelFn f = pick_pair_kernel(c->N, c->att, mode, smem);
+    f<<<grid, 256, sm, c->stream>>>(a);
   } else {
     KernelFn f = pick_kernel(c->N, c->att, pml, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);
@@ -1125,7 +1158,9 @@ int autotune(nexd_ctx* c) {
     const int nel = cls == 0 ? c->Kpml : c->K - c->Kpml;
     if (nel == 0) continue;
     int best = NEXD_CONTRACT_FP32;
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < NKINDS; ++k) {
+      if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N)) continue;
+      if (k == KIND_FP32_PAIRS && (cls == 0 || c->N < 2 || c->N > 5)) continue;
       c->kind[cls] = k;
       if (int st = configure_launch(c)) return st;
       if (int st = time_class(c, cls == 0, 3, c->tune_ms[cls][k])) return st;
@@ -1140,14 +1175,21 @@ int autotune(nexd_ctx* c) {
 
 int nexd_set_contraction(nexd_ctx* c, int32_t mode) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
-  if (mode != NEXD_CONTRACT_FP32 && mode != NEXD_CONTRACT_BF16X3 && mode != NEXD_CONTRACT_AUTO)
+  if (mode != NEXD_CONTRACT_FP32 && mode != NEXD_CONTRACT_BF16X3 && mode != NEXD_CONTRACT_AUTO &&
+      mode != NEXD_CONTRACT_FP32_PAIRS)
     return set_err(c, NEXD_ERR_INVALID, "unknown contraction mode");
-  if (mode != NEXD_CONTRACT_FP32 && !tc_order_supported(c->N))
+  if (mode == NEXD_CONTRACT_FP32_PAIRS && (c->N < 2 || c->N > 5))
+    return set_err(c, NEXD_ERR_UNSUPPORTED, "the node-pair kernel covers orders 2 to 5");
+  if (mode == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N))
     return set_err(c, NEXD_ERR_UNSUPPORTED, "the tensor-core contraction covers order 4");
   const int old[2] = {c->kind[0], c->kind[1]};
   int st;
   if (mode == NEXD_CONTRACT_AUTO) {
     st = autotune(c);
+  } else if (mode == NEXD_CONTRACT_FP32_PAIRS) {
+    c->kind[0] = NEXD_CONTRACT_FP32;
+    c->kind[1] = KIND_FP32_PAIRS;
+    st = configure_launch(c);
   } else {
     c->kind[0] = c->kind[1] = mode;
     st = configure_launch(c);
@@ -1170,7 +1212,7 @@ int nexd_get_contraction(const nexd_ctx* c, int32_t* kinds, float* tune_ms) {
     kinds[1] = c->kind[1];
   }
   if (tune_ms)
-    for (int i = 0; i < 4; ++i) tune_ms[i] = c->tune_ms[i / 2][i % 2];
+    for (int i = 0; i < 2 * NKINDS; ++i) tune_ms[i] = c->tune_ms[i / NKINDS][i % NKINDS];
   return NEXD_OK;
 }
 

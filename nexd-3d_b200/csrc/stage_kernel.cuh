@@ -33,13 +33,17 @@
 
 namespace nexd_dev {
 
-template <int N>
+// Sizes of one order.  NPT nodes per thread: 1 (a thread per node, E =
+// 256 / Np elements per chunk) or 2 (a thread per node pair, twice the
+// elements per chunk).
+template <int N, int NPT = 1>
 struct Order {
   static constexpr int Np = (N + 1) * (N + 2) * (N + 3) / 6;
   static constexpr int NpF = (N + 1) * (N + 2) / 2;
   static constexpr int NF = 4 * NpF;
   static constexpr int THREADS = 256;
-  static constexpr int E = THREADS / Np;  // elements per chunk
+  static constexpr int NPP = (Np + NPT - 1) / NPT;    // threads per element
+  static constexpr int E = NPT * (THREADS / Np);     // elements per chunk
   static constexpr int QS = 12;           // padded field stride of staged q (3 x float4)
   static constexpr int GS = 36;           // per-face expansion coefficients
   static constexpr int CS = 34;           // contravariant-flux row stride (PML): r 0..9, s 10..19, t 20..29
@@ -265,10 +269,9 @@ __device__ __forceinline__ Chunk chunk_of(const StageArgs& a, int w, int nchunk)
 // Asynchronous copies of one chunk's element records (16-byte copies), own
 // wavefield (field-major), the connectivity of the chunk after it (`next`,
 // -1 for none) and the chunk's own face codes.  No commit.
-template <int N>
+template <class O>
 __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, float* bGeo, float* bQ, int* bIds,
                                            const Chunk* next) {
-  using O = Order<N>;
   constexpr int Np = O::Np, E = O::E;
   const int tid = threadIdx.x, nth = blockDim.x;
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
@@ -291,10 +294,9 @@ __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, f
 // Asynchronous gather of the neighbour face traces of one chunk's interior
 // faces through the face patterns, using its connectivity `ids` (staged one
 // chunk earlier).  No commit.
-template <int N>
+template <class O>
 __device__ __forceinline__ void issue_traces(const StageArgs& a, const Chunk& c, const int* ids, float* bTr,
                                              const unsigned char* pat) {
-  using O = Order<N>;
   constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF;
   const int tid = threadIdx.x, nth = blockDim.x;
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
@@ -314,16 +316,15 @@ __device__ __forceinline__ void issue_traces(const StageArgs& a, const Chunk& c,
 
 // All copies of one chunk into a prefetch buffer [records | wavefield |
 // traces | connectivity], committed as one group.
-template <int N>
+template <class O>
 __device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
                                             const Chunk* next, const unsigned char* pat) {
-  using O = Order<N>;
   float* bGeo = buf;
   float* bQ = bGeo + O::SGEO;
   float* bTr = bQ + O::SQF;
   int* bIds = reinterpret_cast<int*>(bTr + O::STR);
-  issue_main<N>(a, c, bGeo, bQ, bIds, next);
-  issue_traces<N>(a, c, ids, bTr, pat);
+  issue_main<O>(a, c, bGeo, bQ, bIds, next);
+  issue_traces<O>(a, c, ids, bTr, pat);
   cp_async_commit();
 }
 
@@ -587,7 +588,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
                                 : reinterpret_cast<const int*>(a.fcode)[4 * (c0.e0 + ee) + k - 4];
     }
     __syncthreads();
-    issue_chunk<N>(a, c0, ids0, sBuf, wn < nwork ? &c1 : nullptr, sPat);
+    issue_chunk<O>(a, c0, ids0, sBuf, wn < nwork ? &c1 : nullptr, sPat);
   }
 
   for (int p = 0; w < nwork; w += gridDim.x, p ^= 1) {
@@ -616,7 +617,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
         const int wnn = wn + gridDim.x;
         Chunk cnn;
         if (wnn < nwork) cnn = chunk_of<E>(a, wnn, nchunk);
-        issue_chunk<N>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, wnn < nwork ? &cnn : nullptr, sPat);
+        issue_chunk<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, wnn < nwork ? &cnn : nullptr, sPat);
       }
     }
     // ---- interleaved own wavefield for the volume loop ------------------------------

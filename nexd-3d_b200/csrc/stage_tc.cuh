@@ -115,8 +115,8 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
                                 : reinterpret_cast<const int*>(a.fcode)[4 * (c0.e0 + ee) + k - 4];
     }
     __syncthreads();
-    issue_main<N>(a, c0, geo_of(0), q_of(0), ids_of(0), wn < nwork ? &c1 : nullptr);
-    issue_traces<N>(a, c0, ids0, sTr, sPat);
+    issue_main<O>(a, c0, geo_of(0), q_of(0), ids_of(0), wn < nwork ? &c1 : nullptr);
+    issue_traces<O>(a, c0, ids0, sTr, sPat);
     cp_async_commit();
   }
 
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
       const int wnn = wn + gridDim.x;
       Chunk cnn;
       if (wnn < nwork) cnn = chunk_of<E>(a, wnn, nchunk);
-      issue_main<N>(a, cn, geo_of(p ^ 1), q_of(p ^ 1), ids_of(p ^ 1), wnn < nwork ? &cnn : nullptr);
+      issue_main<O>(a, cn, geo_of(p ^ 1), q_of(p ^ 1), ids_of(p ^ 1), wnn < nwork ? &cnn : nullptr);
       cp_async_commit();
     }
 
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
     }
     // the face traces of the next chunk (its connectivity arrived with this chunk)
     if (wn < nwork) {
-      issue_traces<N>(a, cn, sIds, sTr, sPat);
+      issue_traces<O>(a, cn, sIds, sTr, sPat);
       cp_async_commit();
     }
 

@@ -77,7 +77,7 @@ class NexdProfile(C.Structure):
                 ("elements", C.c_int64 * NEXD_K_COUNT), ("span_ms", C.c_double)]
 NEXD_STATE_Q, NEXD_STATE_THETA, NEXD_STATE_PML = 0, 1, 2
 NEXD_NOALLOC_MAX_BATCH = 64
-NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3, NEXD_CONTRACT_AUTO = 0, 1, 2
+NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3, NEXD_CONTRACT_AUTO, NEXD_CONTRACT_FP32_PAIRS = 0, 1, 2, 3
 
 _host = None
 _gpu = None

@@ -94,7 +94,7 @@ class Solver:
         "bf16x3" (tcgen05 tensor cores, split BF16, FP32 accumulation) or
         "auto" (the faster of the two per element class, timed on this mesh)."""
         m = {"fp32": _abi.NEXD_CONTRACT_FP32, "bf16x3": _abi.NEXD_CONTRACT_BF16X3,
-             "auto": _abi.NEXD_CONTRACT_AUTO}.get(mode, mode)
+             "auto": _abi.NEXD_CONTRACT_AUTO, "fp32_pairs": _abi.NEXD_CONTRACT_FP32_PAIRS}.get(mode, mode)
         st = _abi.gpu_lib().nexd_set_contraction(self._ctx, m)
         if st != 0:
             raise _gpu_error(self._ctx, st)
@@ -102,13 +102,13 @@ class Solver:
     def contraction(self):
         """({"npml": kind, "rest": kind}, autotune ms per launch {(class, kind): ms})."""
         kinds = (C.c_int32 * 2)()
-        ms = (C.c_float * 4)()
+        ms = (C.c_float * 6)()
         st = _abi.gpu_lib().nexd_get_contraction(self._ctx, kinds, ms)
         if st != 0:
             raise _gpu_error(self._ctx, st)
-        names = {0: "fp32", 1: "bf16x3"}
+        names = {0: "fp32", 1: "bf16x3", 2: "fp32_pairs"}
         return ({"npml": names[kinds[0]], "rest": names[kinds[1]]},
-                {(cl, names[k]): ms[2 * i + k] for i, cl in enumerate(("npml", "rest")) for k in range(2)})
+                {(cl, names[k]): ms[3 * i + k] for i, cl in enumerate(("npml", "rest")) for k in range(3)})
 
     def boundary_faces(self):
         """(elem, face) 1-based arrays of the absorbing faces in ghost-slot order."""

@@ -169,7 +169,34 @@ def test_autotune_leaves_state_and_picks_valid_kinds(tmp_path, oracle, Solver, t
     for x, y in zip(before, after):
         assert np.array_equal(x, y)
     kinds, ms = s.contraction()
-    assert set(kinds.values()) <= {"fp32", "bf16x3"}
-    assert all(v > 0 for v in ms.values())
+    assert set(kinds.values()) <= {"fp32", "bf16x3", "fp32_pairs"}
+    assert kinds["npml"] != "fp32_pairs"
+    # every candidate of each class was timed, the chosen one is the fastest
+    for cl, cands in (("npml", ("fp32", "bf16x3")), ("rest", ("fp32", "bf16x3", "fp32_pairs"))):
+        assert all(ms[(cl, k)] > 0 for k in cands)
+        assert ms[(cl, kinds[cl])] == min(ms[(cl, k)] for k in cands)
     s.run(31, 60)
     assert trace_misfit(s.traces()[..., 0], run_oracle(oracle, m, 64)[..., 0]) < 1e-4
+
+
+@pytest.mark.parametrize("N", [3, 4])
+def test_node_pair_kernel_is_bit_identical(tmp_path, Solver, N):
+    """The node-pair FP32 kernel (elements outside the NPML) performs the
+    FP32 kernel's operations in the same order: identical wavefields, memory
+    variables and traces; AUTO may choose it."""
+    d = str(tmp_path / "pair")
+    synth.write_twolayer(d, cells=(10, 10, 5), nt=12, nrec=4, src_depth=(900.0, 900.0))
+    m = Mesh(d, N=N, stf_stage_time=True)
+    a, b = Solver(m.desc_ptr), Solver(m.desc_ptr)
+    b.set_contraction("fp32_pairs")
+    assert b.contraction()[0] == {"npml": "fp32", "rest": "fp32_pairs"}
+    a.run(1, 12)
+    b.run(1, 12)
+    assert np.array_equal(a.field(), b.field())
+    nth = 6 * m.desc.nMB
+    assert np.array_equal(a.state(_abi.NEXD_STATE_THETA, nfields=nth), b.state(_abi.NEXD_STATE_THETA, nfields=nth))
+    assert np.array_equal(a.traces(), b.traces())
+    c = Solver(m.desc_ptr)
+    c.set_contraction("auto")
+    kinds, ms = c.contraction()
+    assert ms[("rest", "fp32_pairs")] > 0 and ms[("rest", "fp32")] > 0
