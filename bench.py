@@ -67,7 +67,7 @@ WORKLOADS = {
 
 
 def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.5):
-    """Config 5 at training scale: a 2 x 2 x 1 km two-layer model (1,536 tets)
+    """Learned boundary at training scale: a 2 x 2 x 1 km two-layer model (1,536 tets)
     inside an 8-element NPML; train the boundary MLP on n_train sources,
     score plain and learned boundaries against the wide run on n_eval
     held-out sources.  Returns (parameters, summary)."""
@@ -95,7 +95,7 @@ def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.
                "max_reflection": max_reflection,
                "field_err_vs_wide_npml": {"plain": mean("plain", "field_err"), "learned": mean("learned", "field_err")},
                "trace_err_vs_wide_npml": {"plain": mean("plain", "trace_err"), "learned": mean("learned", "trace_err")},
-               "judge": "8-element NPML around the model (the method itself)"}
+               "reference_solution": "8-element NPML around the model (the method itself)"}
     return params, summary
 
 
@@ -114,7 +114,7 @@ def multimodel_specs(seed=4, n=16):
 
 
 def run_multimodel(args, grp, tmp, steps, warmup):
-    """Config 4: the 16 models stepped together as one CUDA graph, grids autotuned."""
+    """16 models of 8,000-300,000 tets stepped together as one CUDA graph, grids autotuned."""
     from nexd_b200.solver import Solver, Group
     import torch
     torch.cuda.set_device(0 if grp.dist is None else grp.local)

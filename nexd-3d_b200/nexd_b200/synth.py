@@ -173,7 +173,7 @@ def write_simulation(directory, *, box, cells, jitter=0.05, seed=1, layers=None,
 
 
 # ---------------------------------------------------------------------------
-# The workloads (sizes and values as the headline configurations state them)
+# The benchmark models (sizes and material values as the benchmark workloads use them)
 # ---------------------------------------------------------------------------
 
 def write_cube(directory, *, cells=10, seed=1, nt=1000):
