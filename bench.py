@@ -67,16 +67,19 @@ WORKLOADS = {
 
 
 def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.5):
-    """Learned boundary at training scale: a 2 x 2 x 1 km two-layer model (1,536 tets)
-    inside an 8-element NPML; train the boundary MLP on n_train sources,
-    score plain and learned boundaries against the wide run on n_eval
-    held-out sources.  Returns (parameters, summary)."""
+    """Learned boundary at training scale: 2 x 2 x 1 km two-layer models (1,536
+    tets) with seeded random layers (vp 2500-5500 m/s, vp/vs 1.6-1.9, rho
+    2200-2900 kg/m^3) inside an 8-element NPML; train the boundary MLP on
+    n_train source/material pairs, score plain and learned boundaries against
+    the wide run on n_eval held-out sources and materials.  Returns
+    (parameters, summary)."""
     from nexd_b200 import boundary
     from nexd_b200.solver import Solver
     cells, h, P, dur = (8, 8, 4), 250.0, 8, 1.2
     srcs = boundary.random_sources(n_train + n_eval, cells, h, seed=seed)
+    mats = boundary.random_layers(n_train + n_eval, cells, h, seed=seed + 12)
     t0 = time.perf_counter()
-    pairs = [boundary.ModelPair(tmp, f"lb{i}", src, cells=cells, h=h, pml_cells=P, duration=dur)
+    pairs = [boundary.ModelPair(tmp, f"lb{i}", src, cells=cells, h=h, pml_cells=P, duration=dur, layers=mats[i])
              for i, src in enumerate(srcs)]
     xs, ys = zip(*(p.training_pairs(Solver, every=2) for p in pairs[:n_train]))
     x, y = np.concatenate(xs), np.concatenate(ys)
@@ -90,7 +93,8 @@ def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.
         res = ev.evaluate(Solver, params, [int(ev.nt * 0.6), int(ev.nt * 0.8), ev.nt], max_reflection=max_reflection)
         scores.append(res)
     mean = lambda k, f: float(np.mean([np.mean(r[k][f]) for r in scores]))
-    summary = {"train_sources": n_train, "heldout_sources": n_eval, "samples": int(len(x)),
+    summary = {"train_sources": n_train, "heldout_sources": n_eval, "materials": "seeded random two-layer",
+               "samples": int(len(x)),
                "loss_first_last": [hist[0], hist[-1]], "data_s": round(t_data, 1), "train_s": round(t_train, 1),
                "max_reflection": max_reflection,
                "field_err_vs_wide_npml": {"plain": mean("plain", "field_err"), "learned": mean("learned", "field_err")},

@@ -255,6 +255,22 @@ def random_sources(n, cells, h, seed, depth=(300.0, 700.0), f0=3.0, margin=2):
     return out
 
 
+def random_layers(n, cells, h, seed, vp=(2500.0, 5500.0), vpvs=(1.6, 1.9), rho=(2200.0, 2900.0)):
+    """n seeded two-layer materials (an upper layer 600 m thick over a
+    half-space), each layer's vp, vp/vs and density uniform in the given
+    ranges; elastic (Q 9000)."""
+    rng = np.random.default_rng(seed)
+    Lz = cells[2] * h
+    out = []
+    for _ in range(n):
+        lay = []
+        for zmin in (Lz - 600.0, -np.inf):
+            p = rng.uniform(*vp)
+            lay.append((zmin, float(p), float(p / rng.uniform(*vpvs)), float(rng.uniform(*rho)), 9000.0, 9000.0))
+        out.append(lay)
+    return out
+
+
 def surface_stations(cells, h, n=9):
     nx, ny, nz = cells
     Lx, Ly, Lz = nx * h, ny * h, nz * h
@@ -267,19 +283,19 @@ def surface_stations(cells, h, n=9):
 class ModelPair:
     """A small (absorbing) model and its wide-NPML extension for one source."""
 
-    def __init__(self, root, name, source, *, cells, h, pml_cells, duration, N=4):
+    def __init__(self, root, name, source, *, cells, h, pml_cells, duration, N=4, layers=None):
         from .host import Mesh
         self.wide_dir = os.path.join(root, f"{name}_wide")
         self.small_dir = os.path.join(root, f"{name}_small")
         st = surface_stations(cells, h)
         # nt from the small model's dt (same tetrahedra, same dt)
         self.map = write_model_pair(self.wide_dir, self.small_dir, cells=cells, h=h, pml_cells=pml_cells, nt=10,
-                                    sources=[source], stations=st)
+                                    sources=[source], stations=st, layers=layers)
         probe = Mesh(self.small_dir, N=N, stf_stage_time=True)
         nt = int(np.ceil(duration / probe.dt))
         probe.close()
         self.map = write_model_pair(self.wide_dir, self.small_dir, cells=cells, h=h, pml_cells=pml_cells, nt=nt,
-                                    sources=[source], stations=st)
+                                    sources=[source], stations=st, layers=layers)
         self.small = Mesh(self.small_dir, N=N, stf_stage_time=True)
         self.wide = Mesh(self.wide_dir, N=N, stf_stage_time=True)
         self.nt = nt
