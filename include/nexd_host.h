@@ -55,6 +55,21 @@ typedef struct nexd_mesh_info {
  * N=4, parfile values, reference t0 and STF sampling, init 1e-24). */
 int nexd_mesh_build(const char* dir, const nexd_build_opts* opts, nexd_mesh** out);
 
+/* Writes the reference's database files for one partition into `outdir`:
+ * meshVar000001 (writeMeshVar, src/meshMod.f90:1401-1504) and, when the mesh
+ * has sources / receivers, srcVar000001 / recVar000001 (writeSrcVar /
+ * writeRecVar, src/sourceReceiverMod.f90:615-648), as Fortran sequential
+ * unformatted records with 4-byte markers, REAL(4) and INTEGER(4) data. */
+int nexd_mesh_write_database(const nexd_mesh* mesh, const char* outdir);
+
+/* Builds the database from `dir`/data/parfile and `dir`/out/{meshVar,srcVar,
+ * recVar}000001 -- the files the reference's mesher writes with nproc = 1 --
+ * as timeloop3D's readMesh / readSrc / readRec do (src/timeloopMod.f90:137-160,
+ * src/meshMod.f90:1506-1640, src/sourceReceiverMod.f90:653-741).  The order
+ * comes from the files (opts->N is ignored); a partition with MPI interfaces
+ * is rejected with NEXD_ERR_INVALID. */
+int nexd_mesh_load_database(const char* dir, const nexd_build_opts* opts, nexd_mesh** out);
+
 /* Descriptor view into the database; valid until nexd_mesh_free. */
 const nexd_desc* nexd_mesh_desc(const nexd_mesh* mesh);
 

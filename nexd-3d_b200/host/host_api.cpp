@@ -21,11 +21,8 @@ int fail(const std::string& msg) {
 }
 }  // namespace
 
-extern "C" {
-
-int nexd_mesh_build(const char* dir, const nexd_build_opts* opts, nexd_mesh** out) {
-  if (!dir || !out) return fail("nexd_mesh_build: null argument");
-  *out = nullptr;
+namespace {
+nexd::BuildOptions to_options(const nexd_build_opts* opts) {
   nexd::BuildOptions o;
   if (opts) {
     if (opts->N > 0) o.N = opts->N;
@@ -37,10 +34,15 @@ int nexd_mesh_build(const char* dir, const nexd_build_opts* opts, nexd_mesh** ou
     o.init_value = opts->init_value;
     o.nbatch = opts->nbatch > 0 ? opts->nbatch : 1;
   }
+  return o;
+}
+
+template <class Build>
+int make_mesh(nexd_mesh** out, Build build) {
   try {
     auto* m = new nexd_mesh;
     try {
-      nexd::build_from_directory(dir, o, m->db);
+      build(m->db);
     } catch (...) {
       delete m;
       throw;
@@ -51,6 +53,33 @@ int nexd_mesh_build(const char* dir, const nexd_build_opts* opts, nexd_mesh** ou
       m->recnr.push_back(r.nr);
     }
     *out = m;
+    return NEXD_OK;
+  } catch (const std::exception& e) {
+    return fail(e.what());
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int nexd_mesh_build(const char* dir, const nexd_build_opts* opts, nexd_mesh** out) {
+  if (!dir || !out) return fail("nexd_mesh_build: null argument");
+  *out = nullptr;
+  const nexd::BuildOptions o = to_options(opts);
+  return make_mesh(out, [&](nexd::MeshDB& db) { nexd::build_from_directory(dir, o, db); });
+}
+
+int nexd_mesh_load_database(const char* dir, const nexd_build_opts* opts, nexd_mesh** out) {
+  if (!dir || !out) return fail("nexd_mesh_load_database: null argument");
+  *out = nullptr;
+  const nexd::BuildOptions o = to_options(opts);
+  return make_mesh(out, [&](nexd::MeshDB& db) { nexd::build_from_database(dir, o, db); });
+}
+
+int nexd_mesh_write_database(const nexd_mesh* mesh, const char* outdir) {
+  if (!mesh || !outdir) return fail("nexd_mesh_write_database: null argument");
+  try {
+    nexd::write_database(mesh->db, outdir);
     return NEXD_OK;
   } catch (const std::exception& e) {
     return fail(e.what());

@@ -458,6 +458,26 @@ static void read_cubit(const std::string& dir, MeshDB& db, std::vector<std::arra
   };
   read_faces("free", freef);
   read_faces("absorb", absf);
+  // material table (optional here; the solver reads per-element values)
+  std::ifstream mp(dir + "/cubit/matprop");
+  if (mp) {
+    mp >> db.nmat;
+    if (!mp || db.nmat < 0) throw std::runtime_error("bad cubit/matprop");
+    db.matval.assign(size_t(db.nmat) * 11, 0.0);
+    for (int i = 0; i < db.nmat; ++i) {
+      double id, dummy, vp, vs, rho, qp, qs;
+      mp >> id >> dummy >> vp >> vs >> rho >> qp >> qs;
+      if (!mp) throw std::runtime_error("truncated cubit/matprop");
+      const size_t n = size_t(db.nmat);
+      db.matval[i] = rho;
+      db.matval[n + i] = vp;
+      db.matval[2 * n + i] = vs;
+      db.matval[3 * n + i] = vs * vs * rho;
+      db.matval[4 * n + i] = vp * vp * rho - 2.0 * vs * vs * rho;
+      db.matval[5 * n + i] = qp;
+      db.matval[6 * n + i] = qs;
+    }
+  }
 }
 
 static void build_topology(MeshDB& db, const std::vector<std::array<int, 4>>& freef,
@@ -885,7 +905,7 @@ static void fill_desc(MeshDB& db) {
   d.srcbatch = db.srcbatch.data();
 }
 
-void build_from_directory(const std::string& dir, const BuildOptions& opt, MeshDB& db) {
+void init_parameters(const std::string& dir, const BuildOptions& opt, MeshDB& db) {
   db = MeshDB{};
   db.opt = opt;
   db.par = read_parfile(dir + "/data/parfile");
@@ -894,6 +914,10 @@ void build_from_directory(const std::string& dir, const BuildOptions& opt, MeshD
   if (opt.nt > 0) db.par.nt = opt.nt;
   if (db.par.timeint < 1 || db.par.timeint > 4) throw std::runtime_error("timeint must be 1..4");
   if (db.par.nt < 1) throw std::runtime_error("nt must be positive");
+}
+
+void build_from_directory(const std::string& dir, const BuildOptions& opt, MeshDB& db) {
+  init_parameters(dir, opt, db);
   db.N = opt.N;
   db.op = build_operators(opt.N);
   db.Np = db.op.Np;
@@ -933,11 +957,15 @@ void build_from_directory(const std::string& dir, const BuildOptions& opt, MeshD
     for (size_t i = 0; i < db.src.size(); ++i) loc.locate(db.src[i].xyz, db.src[i].elem, db.src[i].rst, "source", int(i) + 1);
     for (size_t i = 0; i < db.rec.size(); ++i) loc.locate(db.rec[i].xyz, db.rec[i].elem, db.rec[i].rst, "receiver", int(i) + 1);
   }
+  prepare_solver(db);
+}
+
+void prepare_solver(MeshDB& db) {
   db.f0max = 0.0;
   for (const auto& s : db.src) db.f0max = std::max(db.f0max, s.f0);
   build_pml(db);
   prepare_sources(db);
-  const int Np = db.Np, NpF = db.NpF;
+  const int NpF = db.NpF;
   db.Dr = db.op.Dr.a;
   db.Ds = db.op.Ds.a;
   db.Dt = db.op.Dt.a;
@@ -947,7 +975,6 @@ void build_from_directory(const std::string& dir, const BuildOptions& opt, MeshD
   db.V = db.op.V.a;
   db.fmask1.resize(size_t(NpF) * 4);
   for (size_t i = 0; i < db.fmask1.size(); ++i) db.fmask1[i] = db.op.fmask[i] + 1;
-  (void)Np;
   fill_desc(db);
 }
 

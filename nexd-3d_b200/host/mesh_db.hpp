@@ -62,6 +62,8 @@ struct MeshDB {
   std::vector<int> neighbor;  // (4,K) 1-based, 0 boundary
   std::vector<int> face;      // (4,K)
   std::vector<int> mat, pml;  // (K)
+  int nmat = 0;
+  std::vector<double> matval;  // (nmat,11): rho vp vs mu lambda qp qs (cubit/matprop, src/meshMod.f90:261-272)
   std::vector<double> vp, vs, rho, qp, qs, mu, lambda, vpu, vsu, muu, lambdau;  // (K)
   std::vector<double> ylambda, ymu;  // (nMB,K)
   std::vector<double> wl, wk;
@@ -93,6 +95,25 @@ struct MeshDB {
 // Throws std::runtime_error with a message on any inconsistency the reference
 // mesher would stop on.
 void build_from_directory(const std::string& dir, const BuildOptions& opt, MeshDB& db);
+
+// Reads data/parfile of `dir` into db.par and applies the option overrides.
+void init_parameters(const std::string& dir, const BuildOptions& opt, MeshDB& db);
+
+// Solver-side set-up once mesh, sources and receivers are known: NPML
+// profiles, source/receiver interpolation and STF tables, operators in the
+// descriptor (src/timeloopMod.f90:137-356).
+void prepare_solver(MeshDB& db);
+
+// Database files of the reference's mesher -> solver hand-off for one
+// partition (nproc = 1): out/meshVar000001 (writeMeshVar / readMeshVar,
+// src/meshMod.f90:1401-1640), srcVar000001 / recVar000001 (writeSrcVar,
+// writeRecVar, readSrcVar, readRecVar, src/sourceReceiverMod.f90:615-702),
+// as Fortran sequential unformatted records.
+void write_database(const MeshDB& db, const std::string& outdir);
+// Builds the database from `dir`/data/parfile and the files above in
+// `dir`/out, as the reference's timeloop3D does with readMesh / readSrc /
+// readRec (src/timeloopMod.f90:137-160).  The order comes from the files.
+void build_from_database(const std::string& dir, const BuildOptions& opt, MeshDB& db);
 
 // Parfile / source-file readers (src/parameterMod.f90, src/fileParameterMod.f90,
 // src/sourceReceiverMod.f90:36-201).

@@ -60,7 +60,7 @@ class NexdMeshInfo(C.Structure):
 
 # Entry points declared in include/*.h, per library (checked by the CPU tests).
 HOST_SYMBOLS = ["nexd_mesh_build", "nexd_mesh_desc", "nexd_mesh_get_info", "nexd_mesh_write_seismograms",
-                "nexd_mesh_last_error", "nexd_mesh_free"]
+                "nexd_mesh_last_error", "nexd_mesh_free", "nexd_mesh_write_database", "nexd_mesh_load_database"]
 GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
                "nexd_get_state", "nexd_set_state", "nexd_step_io", "nexd_pml_trigger", "nexd_get_energy",
                "nexd_set_contraction", "nexd_get_contraction", "nexd_boundary_faces", "nexd_set_boundary_mlp",
@@ -96,6 +96,10 @@ def host_lib():
         lib = _load("libnexd_host.so")
         lib.nexd_mesh_build.argtypes = [C.c_char_p, C.POINTER(NexdBuildOpts), C.POINTER(C.c_void_p)]
         lib.nexd_mesh_build.restype = C.c_int
+        lib.nexd_mesh_load_database.argtypes = [C.c_char_p, C.POINTER(NexdBuildOpts), C.POINTER(C.c_void_p)]
+        lib.nexd_mesh_load_database.restype = C.c_int
+        lib.nexd_mesh_write_database.argtypes = [C.c_void_p, C.c_char_p]
+        lib.nexd_mesh_write_database.restype = C.c_int
         lib.nexd_mesh_desc.argtypes = [C.c_void_p]
         lib.nexd_mesh_desc.restype = C.POINTER(NexdDesc)
         lib.nexd_mesh_get_info.argtypes = [C.c_void_p, C.POINTER(NexdMeshInfo)]

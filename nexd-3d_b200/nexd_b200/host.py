@@ -1,6 +1,7 @@
 """Host-side mesh database (libnexd_host.so): the single-partition NEXD-3D
 mesher and solver set-up that produce the nexd_desc of the C-ABI."""
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -37,13 +38,17 @@ class Mesh:
     """
 
     def __init__(self, directory, N=4, timeint=0, cfl=0.0, nt=0, t0=0.0, stf_stage_time=False,
-                 init_value=1e-24, nbatch=1):
+                 init_value=1e-24, nbatch=1, database=False):
+        """database=True reads directory/out/{meshVar,srcVar,recVar}000001 (the
+        reference mesher's output for one partition; the order comes from the
+        files) instead of running the mesher on directory/cubit."""
         lib = _abi.host_lib()
         opts = _abi.NexdBuildOpts(N=N, timeint=timeint, cfl=cfl, nt=nt, t0=t0,
                                   stf_stage_time=1 if stf_stage_time else 0, init_value=init_value,
                                   nbatch=nbatch)
         h = C.c_void_p()
-        st = lib.nexd_mesh_build(str(directory).encode(), C.byref(opts), C.byref(h))
+        build = lib.nexd_mesh_load_database if database else lib.nexd_mesh_build
+        st = build(str(directory).encode(), C.byref(opts), C.byref(h))
         if st != 0:
             raise _host_error(st)
         self._h = h
@@ -84,6 +89,14 @@ class Mesh:
         if name == "recnr":
             return _arr(info.recnr, (d.nrec,), np.int32)
         raise KeyError(name)
+
+    def write_database(self, outdir):
+        """Writes meshVar000001 (+ srcVar000001 / recVar000001) into outdir as
+        the reference's mesher does for one partition."""
+        os.makedirs(outdir, exist_ok=True)
+        st = _abi.host_lib().nexd_mesh_write_database(self._h, str(outdir).encode())
+        if st != 0:
+            raise _host_error(st)
 
     def write_seismograms(self, outdir, traces, nt_written=None, batch=0):
         tr = np.asfortranarray(traces, dtype=np.float32)

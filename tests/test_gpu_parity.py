@@ -143,6 +143,25 @@ def test_brick_golden_on_gpu(tmp_path, Solver):
     assert trace_misfit(tr, golden) < 1e-4
 
 
+def test_brick_golden_from_database_files_on_gpu(tmp_path, Solver):
+    """The brick example handed over as the reference's database files
+    (meshVar000001, srcVar000001, recVar000001: REAL(4) records, read as
+    timeloop3D's readMesh / readSrc / readRec do) reproduces the golden
+    seismograms on the GPU within the same bounds."""
+    golden, _ = write_brick(str(tmp_path))
+    Mesh(str(tmp_path), N=4).write_database(str(tmp_path / "out"))
+    # the reference's dt = 6.46257467e-06 from the REAL(4) dtfactor of the file
+    dtf = Mesh(str(tmp_path), database=True).info.dtfactor
+    m = Mesh(str(tmp_path), database=True, cfl=6.46257467e-06 / dtf)
+    assert m.N == 4 and abs(m.dt - 6.46257467e-06) < 1e-14
+    pin_brick_edge_stations(m)
+    s = Solver(m.desc_ptr)
+    s.run(1, 1000)
+    tr = s.traces()[..., 0]
+    assert station_misfit(tr, golden) < 2e-4
+    assert trace_misfit(tr, golden) < 1e-4
+
+
 def test_batched_wavefields(tmp_path, Solver):
     """nbatch independent wavefields in one launch equal separate runs."""
     d = str(tmp_path / "b")
