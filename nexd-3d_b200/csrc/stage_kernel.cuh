@@ -60,16 +60,26 @@ struct Order {
   static constexpr int STR = r4(E * NF * 9);
   static constexpr int SIDS = r4(E * 12);
   static constexpr int BUF = SGEO + SQF + STR + SIDS;
-  // per-element strides of the work areas are = 16 (mod 32) words, so the two
-  // elements that share a warp read different shared-memory banks
-  static constexpr int b16(int x) { return x + ((16 - x % 32) + 32) % 32; }
-  static constexpr int QE = b16(Np * QS);   // interleaved own wavefield per element
-  static constexpr int CFE = b16(Np * CS);  // contravariant fluxes per element (PML)
-  static constexpr int AE = b16(3 * NFP);   // amplitudes per element
+  // Warp-aligned node mapping (one node per thread, Np > 32): each of the
+  // first E warps holds nodes 0..31 of one element and the remaining nodes of
+  // all elements share the last warps, so no warp holds node n of one element
+  // and node n+32 of another (the same bank of a Dr/Ds/Dt or LIFT row).
+  static constexpr bool WARP_ALIGNED = NPT == 1 && Np > 32;
+  // smallest x' >= x with x' = m (mod 32)
+  static constexpr int at_bank(int x, int m) { return x + ((m - x % 32) + 32) % 32; }
+  // Per-element strides of the work areas put the elements that share a warp
+  // on different banks: = 16 (mod 32) words for two elements per warp; with
+  // the warp-aligned mapping up to E elements share the last warp, and
+  // strides of 4 (16-byte loads) or 2 (8-byte loads) words keep them apart.
+  static constexpr int b16(int x) { return at_bank(x, 16); }
+  static constexpr int QE = WARP_ALIGNED ? at_bank(Np * QS, 4) : b16(Np * QS);  // interleaved own wavefield
+  static constexpr int CFE = WARP_ALIGNED ? at_bank(Np * CS, 2) : b16(Np * CS);  // contravariant fluxes (PML)
+  static constexpr int AE = WARP_ALIGNED ? at_bank(3 * NFP, 2) : b16(3 * NFP);  // amplitudes per element
+  static constexpr int GE = WARP_ALIGNED ? at_bank(4 * GS, 4) : 4 * GS;  // face coefficients per element
   static constexpr int SQI = E * QE;        // interleaved copy for the volume loop (non-PML)
-  static constexpr int SAMP = E * AE;       // amplitudes [e][comp][padded face node]
-  static constexpr int SG = E * 4 * GS;
-  static constexpr int SCF = E * CFE;
+  static constexpr int SAMP = r4(E * AE);   // amplitudes [e][comp][padded face node]
+  static constexpr int SG = E * GE;
+  static constexpr int SCF = r4(E * CFE);
   static constexpr int SPAT = r4(64 * NpF / 4 + 1);  // face patterns (bytes/4), up to 64 rows
   static constexpr int smem_floats(bool pml) {
     return SD + SL + 2 * BUF + (pml ? SCF : SQI) + SAMP + SG + SPAT;
@@ -570,8 +580,20 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
   const int nel = a.e_end - a.e_begin;
   const int nchunk = (nel + E - 1) / E;
   const int nwork = nchunk * a.nbatch;
-  const int le = tid / Np;       // element of this thread within the chunk
-  const int n = tid - le * Np;   // node of this thread
+  int le, n;  // element of this thread within the chunk, node of this thread
+  if constexpr (O::WARP_ALIGNED) {
+    if (tid < E * 32) {
+      le = tid >> 5;
+      n = tid & 31;
+    } else {
+      const int r = tid - E * 32;
+      le = r / (Np - 32);
+      n = 32 + r - le * (Np - 32);
+    }
+  } else {
+    le = tid / Np;
+    n = tid - le * Np;
+  }
   int w = blockIdx.x;
   if (w >= nwork) return;
 
@@ -644,7 +666,8 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       am[O::NFP] = as1 * fs;
       am[2 * O::NFP] = as2 * fs;
     }
-    for (int i = tid; i < ne * 4; i += blockDim.x) face_coeffs(sGeo + (i >> 2) * GEO_STRIDE, i & 3, sG + i * GS);
+    for (int i = tid; i < ne * 4; i += blockDim.x)
+      face_coeffs(sGeo + (i >> 2) * GEO_STRIDE, i & 3, sG + (i >> 2) * O::GE + (i & 3) * GS);
 
     // ---- PML: auxiliary update and contravariant modified fluxes ------------------
     float vgrad[9];  // d(v_c)/d(x_d) [c*3+d] (anelastic)
@@ -786,7 +809,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
         c2 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + 2 * O::NFP + 2 * ip), c2);
       }
       const float A0 = c0.x + c0.y, A1 = c1.x + c1.y, A2 = c2.x + c2.y;
-      const float4* G4 = reinterpret_cast<const float4*>(sG + (le * 4 + f) * GS);
+      const float4* G4 = reinterpret_cast<const float4*>(sG + le * O::GE + f * GS);
       const float4 g0 = G4[0], g1 = G4[1], g2 = G4[2], g3 = G4[3], g4 = G4[4], g5 = G4[5], g6 = G4[6];
       const float G[28] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w, g2.x, g2.y, g2.z, g2.w, g3.x, g3.y,
                            g3.z, g3.w, g4.x, g4.y, g4.z, g4.w, g5.x, g5.y, g5.z, g5.w, g6.x, g6.y, g6.z, g6.w};

@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
       am[O::NFP] = as1 * fs;
       am[2 * O::NFP] = as2 * fs;
     }
-    for (int i = tid; i < ne * 4; i += blockDim.x) face_coeffs(sGeo + (i >> 2) * GEO_STRIDE, i & 3, sG + i * GS);
+    for (int i = tid; i < ne * 4; i += blockDim.x)
+      face_coeffs(sGeo + (i >> 2) * GEO_STRIDE, i & 3, sG + (i >> 2) * O::GE + (i & 3) * GS);
     __syncthreads();
     if (!active) continue;
 
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
         s1 = __ffma2_rn(l2, u1, s1);
         s2 = __ffma2_rn(l2, u2, s2);
       }
-      const float4* G4 = reinterpret_cast<const float4*>(sG + (le * 4 + f) * GS);
+      const float4* G4 = reinterpret_cast<const float4*>(sG + le * O::GE + f * GS);
       lift_expand<ATT>(G4, p0.x + p0.y, p1.x + p1.y, p2.x + p2.y, as, rq1, sa1);
       lift_expand<ATT>(G4, s0.x + s0.y, s1.x + s1.y, s2.x + s2.y, as, rq2, sa2);
     }
