@@ -10,7 +10,8 @@ fields count).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload twolayer|cube|batch64|multimodel|learned]
-                  [--contraction fp32|bf16x3|auto]
+                  [--contraction fp32|bf16x3|auto|fp32_pairs]
+                  [--kernels npml=KIND,rest=KIND]   (pinned per-class kernels)
 
 Other workloads (measurements beside the headline, not the headline):
   cube     homogeneous elastic 2 km cube, 6,000 tets, N=3, absorbing sides,
@@ -286,6 +287,10 @@ def main():
     ap.add_argument("--contraction", default="auto", choices=["fp32", "bf16x3", "auto", "fp32_pairs"],
                     help="element contraction: FP32 CUDA cores, split-BF16 tcgen05 tensor cores, or the faster "
                          "per element class (timed before the run)")
+    ap.add_argument("--kernels", default=None,
+                    help="pin the kernel per element class instead of --contraction, e.g. npml=bf16x3,rest=fp32 "
+                         "(the choice an auto run reports in kernels_per_class; profiled runs use it, since "
+                         "timing under a profiler would change the auto choice)")
     ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
     ap.add_argument("--cells", default=None, help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
     args = ap.parse_args()
@@ -339,7 +344,12 @@ def main():
             mesh = Mesh(d, N=wl["N"], stf_stage_time=True, nbatch=nsrc)
         s = Solver(mesh.desc_ptr)
         contraction = args.contraction if (mesh.N == 4 or args.contraction != "bf16x3") else "fp32"
-        s.set_contraction(contraction)  # the tensor-core kernels cover N=4
+        if args.kernels:
+            pinned = dict(kv.split("=") for kv in args.kernels.split(","))
+            s.set_contraction_kinds(pinned["npml"], pinned["rest"])
+            contraction = "pinned " + args.kernels
+        else:
+            s.set_contraction(contraction)  # the tensor-core kernels cover N=4
         if learned is not None:
             s.set_boundary_mlp(lb_params, learned["max_reflection"])
         nstage = 5

@@ -264,6 +264,14 @@ int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
  * tune_ms[class * 3 + kind] (0 where not measured).  Either pointer may be NULL. */
 int nexd_get_contraction(const nexd_ctx* ctx, int32_t* kinds, float* tune_ms);
 
+/* Pins the kernel per element class without timing: kinds[0] for NPML
+ * elements (NEXD_CONTRACT_FP32 or NEXD_CONTRACT_BF16X3), kinds[1] for the rest
+ * (those two or 2 = the node-pair FP32 kernel), as nexd_get_contraction
+ * reports them -- e.g. to replay an earlier AUTO choice, so that repeated or
+ * profiled runs use the same kernels.  NEXD_ERR_UNSUPPORTED for a kind the
+ * order lacks, NEXD_ERR_INVALID for an unknown kind. */
+int nexd_set_contraction_kinds(nexd_ctx* ctx, const int32_t* kinds);
+
 /* ---- Movie snapshots (src/timeloopMod.f90:482-489, 576-581; collectMovieMod.f90) ----
  * With frame > 0 every step integrates the displacement u += dt v at every
  * node on the device (from the start value, 1e-24 in the reference) and every

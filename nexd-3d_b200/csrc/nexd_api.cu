@@ -1205,6 +1205,30 @@ int nexd_set_contraction(nexd_ctx* c, int32_t mode) {
   return NEXD_OK;
 }
 
+int nexd_set_contraction_kinds(nexd_ctx* c, const int32_t* kinds) {
+  if (!c || !kinds) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  for (int cls = 0; cls < 2; ++cls) {
+    const int k = kinds[cls];
+    if (k != NEXD_CONTRACT_FP32 && k != NEXD_CONTRACT_BF16X3 && !(cls == 1 && k == KIND_FP32_PAIRS))
+      return set_err(c, NEXD_ERR_INVALID, "unknown kernel kind for this element class");
+    if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N))
+      return set_err(c, NEXD_ERR_UNSUPPORTED, "the tensor-core contraction covers order 4");
+    if (k == KIND_FP32_PAIRS && (c->N < 2 || c->N > 5))
+      return set_err(c, NEXD_ERR_UNSUPPORTED, "the node-pair kernel covers orders 2 to 5");
+  }
+  const int old[2] = {c->kind[0], c->kind[1]};
+  c->kind[0] = kinds[0];
+  c->kind[1] = kinds[1];
+  if (const int st = configure_launch(c)) {
+    c->kind[0] = old[0];
+    c->kind[1] = old[1];
+    configure_launch(c);
+    return st;
+  }
+  drop_graphs(c);
+  return NEXD_OK;
+}
+
 int nexd_get_contraction(const nexd_ctx* c, int32_t* kinds, float* tune_ms) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
   if (kinds) {

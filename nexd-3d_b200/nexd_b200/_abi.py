@@ -63,7 +63,7 @@ HOST_SYMBOLS = ["nexd_mesh_build", "nexd_mesh_desc", "nexd_mesh_get_info", "nexd
                 "nexd_mesh_last_error", "nexd_mesh_free", "nexd_mesh_write_database", "nexd_mesh_load_database"]
 GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
                "nexd_get_state", "nexd_set_state", "nexd_step_io", "nexd_pml_trigger", "nexd_get_energy",
-               "nexd_set_contraction", "nexd_get_contraction", "nexd_boundary_faces", "nexd_set_boundary_mlp",
+               "nexd_set_contraction", "nexd_get_contraction", "nexd_set_contraction_kinds", "nexd_boundary_faces", "nexd_set_boundary_mlp",
                "nexd_get_ghost", "nexd_get_face_traces", "nexd_mlp_param_count", "nexd_mlp_workspace_floats",
                "nexd_mlp_forward", "nexd_mlp_loss_grad", "nexd_mlp_adam", "nexd_group_create", "nexd_group_run",
                "nexd_group_autotune", "nexd_group_span", "nexd_group_destroy", "nexd_movie", "nexd_get_movie",
@@ -132,6 +132,7 @@ def gpu_lib():
         lib.nexd_get_energy.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.nexd_set_contraction.argtypes = [vp, C.c_int32]
         lib.nexd_get_contraction.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
+        lib.nexd_set_contraction_kinds.argtypes = [vp, C.POINTER(C.c_int32)]
         i32p = C.POINTER(C.c_int32)
         lib.nexd_boundary_faces.argtypes = [vp, i32p, i32p, i32p]
         lib.nexd_set_boundary_mlp.argtypes = [vp, C.POINTER(C.c_float), C.c_int64, C.c_float]

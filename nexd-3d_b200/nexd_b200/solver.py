@@ -99,6 +99,15 @@ class Solver:
         if st != 0:
             raise _gpu_error(self._ctx, st)
 
+    def set_contraction_kinds(self, npml, rest):
+        """Pins the kernel per element class ("fp32", "bf16x3", "fp32_pairs"
+        for the rest), e.g. an earlier auto choice, without timing."""
+        m = {"fp32": 0, "bf16x3": 1, "fp32_pairs": 2}
+        kinds = (C.c_int32 * 2)(m.get(npml, npml), m.get(rest, rest))
+        st = _abi.gpu_lib().nexd_set_contraction_kinds(self._ctx, kinds)
+        if st != 0:
+            raise _gpu_error(self._ctx, st)
+
     def contraction(self):
         """({"npml": kind, "rest": kind}, autotune ms per launch {(class, kind): ms})."""
         kinds = (C.c_int32 * 2)()

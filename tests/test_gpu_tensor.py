@@ -200,3 +200,37 @@ def test_node_pair_kernel_is_bit_identical(tmp_path, Solver, N):
     c.set_contraction("auto")
     kinds, ms = c.contraction()
     assert ms[("rest", "fp32_pairs")] > 0 and ms[("rest", "fp32")] > 0
+
+
+def test_pinned_kernel_kinds(tmp_path, oracle, Solver):
+    """nexd_set_contraction_kinds pins the kernel per element class without
+    timing: the pinned FP32 / node-pair pair is bit-identical to the FP32
+    path, the tensor-core NPML kernel stays within the FP32 tolerance of the
+    oracle, and kinds the class or order lacks are refused."""
+    d = str(tmp_path / "pin")
+    synth.write_twolayer(d, cells=(8, 8, 4), nt=40, nrec=6, src_depth=(900.0, 900.0))
+    m = Mesh(d, N=4, stf_stage_time=True)
+    ref = Solver(m.desc_ptr)
+    ref.run(1, 40)
+    a = Solver(m.desc_ptr)
+    a.set_contraction_kinds("fp32", "fp32_pairs")
+    assert a.contraction()[0] == {"npml": "fp32", "rest": "fp32_pairs"}
+    a.run(1, 40)
+    assert np.array_equal(a.traces(), ref.traces())
+    b = Solver(m.desc_ptr)
+    b.set_contraction_kinds("bf16x3", "fp32")
+    assert b.contraction()[0] == {"npml": "bf16x3", "rest": "fp32"}
+    b.run(1, 40)
+    assert trace_misfit(b.traces()[..., 0], run_oracle(oracle, m, 64)[..., 0]) < 1e-4
+    with pytest.raises(NexdError) as ei:
+        b.set_contraction_kinds("fp32_pairs", "fp32")  # no node-pair kernel for NPML elements
+    assert ei.value.status == _abi.NEXD_ERR_INVALID
+    assert b.contraction()[0] == {"npml": "bf16x3", "rest": "fp32"}  # unchanged
+    d3 = str(tmp_path / "n3")
+    synth.write_cube(d3, cells=3, nt=4)
+    m3 = Mesh(d3, N=3)
+    s3 = Solver(m3.desc_ptr)
+    with pytest.raises(NexdError) as ei:
+        s3.set_contraction_kinds("fp32", "bf16x3")
+    assert ei.value.status == _abi.NEXD_ERR_UNSUPPORTED
+    s3.run(1, 4)
