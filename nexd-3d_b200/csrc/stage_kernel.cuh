@@ -697,24 +697,30 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     // ---- volume term ------------------------------------------------------------
     if (!PML) {
       // d/dr, d/ds, d/dt of the 9 fields as packed pairs (fields 2j, 2j+1; pair 4 = field 8 + pad)
-      float2 ar[5], as_[5], at[5];
+      // fields 0..7 as packed pairs, field 8 as scalars (its 4-byte load is one
+      // shared-memory wavefront, a padded pair two)
+      float2 ar[4], as_[4], at[4];
+      float r8 = 0.f, s8 = 0.f, t8 = 0.f;
 #pragma unroll
-      for (int j = 0; j < 5; ++j) { ar[j] = make_float2(0.f, 0.f); as_[j] = ar[j]; at[j] = ar[j]; }
+      for (int j = 0; j < 4; ++j) { ar[j] = make_float2(0.f, 0.f); as_[j] = ar[j]; at[j] = ar[j]; }
       const float* qe = sQI + le * O::QE;
 #pragma unroll 5
       for (int k = 0; k < Np; ++k) {
         const float dx = sD[k * Np + n], dy = sD[Np * Np + k * Np + n], dz = sD[2 * Np * Np + k * Np + n];
         const float2 d0 = make_float2(dx, dx), d1 = make_float2(dy, dy), d2 = make_float2(dz, dz);
         const float4 qa = ld4(qe + k * QS), qb = ld4(qe + k * QS + 4);
-        const float2 qc = *reinterpret_cast<const float2*>(qe + k * QS + 8);
-        const float2 qp[5] = {make_float2(qa.x, qa.y), make_float2(qa.z, qa.w), make_float2(qb.x, qb.y),
-                              make_float2(qb.z, qb.w), qc};
+        const float q8 = qe[k * QS + 8];
+        const float2 qp[4] = {make_float2(qa.x, qa.y), make_float2(qa.z, qa.w), make_float2(qb.x, qb.y),
+                              make_float2(qb.z, qb.w)};
 #pragma unroll
-        for (int j = 0; j < 5; ++j) {
+        for (int j = 0; j < 4; ++j) {
           ar[j] = __ffma2_rn(d0, qp[j], ar[j]);
           as_[j] = __ffma2_rn(d1, qp[j], as_[j]);
           at[j] = __ffma2_rn(d2, qp[j], at[j]);
         }
+        r8 = fmaf(dx, q8, r8);
+        s8 = fmaf(dy, q8, s8);
+        t8 = fmaf(dz, q8, t8);
       }
       float dr[9], ds[9], dtt[9];
 #pragma unroll
@@ -723,7 +729,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
         ds[2 * j] = as_[j].x; ds[2 * j + 1] = as_[j].y;
         dtt[2 * j] = at[j].x; dtt[2 * j + 1] = at[j].y;
       }
-      dr[8] = ar[4].x; ds[8] = as_[4].x; dtt[8] = at[4].x;
+      dr[8] = r8; ds[8] = s8; dtt[8] = t8;
       const float rx = g[G_RX], ry = g[G_RY], rz = g[G_RZ], sx = g[G_SX], sy = g[G_SY], sz = g[G_SZ],
                   tx = g[G_TX], ty = g[G_TY], tz = g[G_TZ];
 #define DX(c) (rx * dr[c] + sx * ds[c] + tx * dtt[c])
