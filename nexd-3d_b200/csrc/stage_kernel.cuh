@@ -75,14 +75,12 @@ struct Order {
   static constexpr int QE = WARP_ALIGNED ? at_bank(Np * QS, 4) : b16(Np * QS);  // interleaved own wavefield
   static constexpr int CFE = WARP_ALIGNED ? at_bank(Np * CS, 2) : b16(Np * CS);  // contravariant fluxes (PML)
   static constexpr int AE = WARP_ALIGNED ? at_bank(3 * NFP, 2) : b16(3 * NFP);  // amplitudes per element
-  static constexpr int GE = WARP_ALIGNED ? at_bank(4 * GS, 4) : 4 * GS;  // face coefficients per element
   static constexpr int SQI = E * QE;        // interleaved copy for the volume loop (non-PML)
   static constexpr int SAMP = r4(E * AE);   // amplitudes [e][comp][padded face node]
-  static constexpr int SG = E * GE;
   static constexpr int SCF = r4(E * CFE);
   static constexpr int SPAT = r4(64 * NpF / 4 + 1);  // face patterns (bytes/4), up to 64 rows
   static constexpr int smem_floats(bool pml) {
-    return SD + SL + 2 * BUF + (pml ? SCF : SQI) + SAMP + SG + SPAT;
+    return SD + SL + 2 * BUF + (pml ? SCF : SQI) + SAMP + SPAT;
   }
 };
 
@@ -220,6 +218,46 @@ __device__ __forceinline__ void face_coeffs(const float* g, int f, float* out) {
   out[27] = nx * nx * ap; out[28] = ny * ny * ap; out[29] = nz * nz * ap;
   out[30] = nx * ny * ap; out[31] = ny * nz * ap; out[32] = nx * nz * ap;
   out[33] = 0.f; out[34] = 0.f; out[35] = 0.f;
+}
+
+// Lifted upwind flux of face f expanded to the 9 fields and the anelastic
+// stress flux, from the lifted amplitudes A0 (P), A1, A2 (S along s, t).  The
+// rank-3 form A0 [n n^T + c (s s^T + t t^T)] + A1 (n s^T + s n^T) +
+// A2 (n t^T + t n^T) of face_coeffs is evaluated with s s^T + t t^T = I - n n^T
+// ((n, s, t) orthonormal) as n v^T + v n^T + c A0 I, v = (1-c)/2 A0 n + m,
+// m = A1 s + A2 t; velocity -(A0 n / Zp + m / Zs); anelastic
+// A0 n n^T / (lambda+2mu) + (n m^T + m n^T) / (2 mu) = n u^T + u n^T.
+// Reads 9 words of the element record per face instead of 36 coefficients.
+template <bool ATT>
+__device__ __forceinline__ void face_expand(const float* g, int f, float A0, float A1, float A2, float* rq,
+                                            float* sig_an) {
+  const float n0 = g[G_N + 3 * f], n1 = g[G_N + 3 * f + 1], n2 = g[G_N + 3 * f + 2];
+  const float m0 = A1 * g[G_S + 3 * f] + A2 * g[G_T + 3 * f];
+  const float m1 = A1 * g[G_S + 3 * f + 1] + A2 * g[G_T + 3 * f + 1];
+  const float m2 = A1 * g[G_S + 3 * f + 2] + A2 * g[G_T + 3 * f + 2];
+  const float c = g[G_C];
+  const float h = 0.5f * (1.f - c) * A0, b = c * A0;
+  const float v0 = fmaf(h, n0, m0), v1 = fmaf(h, n1, m1), v2 = fmaf(h, n2, m2);
+  rq[0] += fmaf(2.f * n0, v0, b);
+  rq[1] += fmaf(2.f * n1, v1, b);
+  rq[2] += fmaf(2.f * n2, v2, b);
+  rq[3] += n0 * v1 + v0 * n1;
+  rq[4] += n1 * v2 + v1 * n2;
+  rq[5] += n0 * v2 + v0 * n2;
+  const float p = g[G_IZP] * A0, q = g[G_IZS];
+  rq[6] -= fmaf(p, n0, q * m0);
+  rq[7] -= fmaf(p, n1, q * m1);
+  rq[8] -= fmaf(p, n2, q * m2);
+  if (ATT) {
+    const float ha = 0.5f * g[G_AP] * A0, as = g[G_AS];
+    const float u0 = fmaf(ha, n0, as * m0), u1 = fmaf(ha, n1, as * m1), u2 = fmaf(ha, n2, as * m2);
+    sig_an[0] += 2.f * n0 * u0;
+    sig_an[1] += 2.f * n1 * u1;
+    sig_an[2] += 2.f * n2 * u2;
+    sig_an[3] += n0 * u1 + u0 * n1;
+    sig_an[4] += n1 * u2 + u1 * n2;
+    sig_an[5] += n0 * u2 + u0 * n2;
+  }
 }
 
 // Characteristic amplitudes (a_p, a_s1, a_s2) of the upwind flux at one face
@@ -557,7 +595,7 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
 template <int N, bool ATT, bool PML, int MODE>
 __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs a) {
   using O = Order<N>;
-  constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, QS = O::QS, GS = O::GS, CS = O::CS;
+  constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, QS = O::QS, CS = O::CS;
   extern __shared__ __align__(16) float smem[];
   float* sD = smem;              // 3*Np*Np: D[d][k][n]
   float* sL = sD + O::SD;        // LIFT in face-node pairs
@@ -565,8 +603,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
   float* sQI = sBuf + 2 * O::BUF;  // non-PML: interleaved own wavefield [e][k][QS]
   float* sCF = sQI;              // PML: contravariant modified fluxes [e][k][CS]
   float* sAmp = sQI + (PML ? O::SCF : O::SQI);  // E*3*NFP
-  float* sG = sAmp + O::SAMP;    // E*4*GS
-  unsigned char* sPat = reinterpret_cast<unsigned char*>(sG + O::SG);  // face patterns
+  unsigned char* sPat = reinterpret_cast<unsigned char*>(sAmp + O::SAMP);  // face patterns
 
   const int tid = threadIdx.x;
   for (int i = tid; i < 3 * Np * Np; i += blockDim.x) sD[i] = a.D[i];
@@ -666,8 +703,6 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       am[O::NFP] = as1 * fs;
       am[2 * O::NFP] = as2 * fs;
     }
-    for (int i = tid; i < ne * 4; i += blockDim.x)
-      face_coeffs(sGeo + (i >> 2) * GEO_STRIDE, i & 3, sG + (i >> 2) * O::GE + (i & 3) * GS);
 
     // ---- PML: auxiliary update and contravariant modified fluxes ------------------
     float vgrad[9];  // d(v_c)/d(x_d) [c*3+d] (anelastic)
@@ -814,26 +849,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
         c1 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + O::NFP + 2 * ip), c1);
         c2 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + 2 * O::NFP + 2 * ip), c2);
       }
-      const float A0 = c0.x + c0.y, A1 = c1.x + c1.y, A2 = c2.x + c2.y;
-      const float4* G4 = reinterpret_cast<const float4*>(sG + le * O::GE + f * GS);
-      const float4 g0 = G4[0], g1 = G4[1], g2 = G4[2], g3 = G4[3], g4 = G4[4], g5 = G4[5], g6 = G4[6];
-      const float G[28] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w, g2.x, g2.y, g2.z, g2.w, g3.x, g3.y,
-                           g3.z, g3.w, g4.x, g4.y, g4.z, g4.w, g5.x, g5.y, g5.z, g5.w, g6.x, g6.y, g6.z, g6.w};
-      float X[6];
-#pragma unroll
-      for (int c = 0; c < 6; ++c) X[c] = G[6 + c] * A1 + G[12 + c] * A2;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) rq[c] += G[c] * A0 + X[c];
-      rq[6] += G[18] * A0 + G[21] * A1 + G[24] * A2;
-      rq[7] += G[19] * A0 + G[22] * A1 + G[25] * A2;
-      rq[8] += G[20] * A0 + G[23] * A1 + G[26] * A2;
-      if (ATT) {
-        const float as = g[G_AS];
-        const float4 g7 = G4[7], g8 = G4[8];
-        const float NN[6] = {G[27], g7.x, g7.y, g7.z, g7.w, g8.x};
-#pragma unroll
-        for (int c = 0; c < 6; ++c) sig_an[c] += NN[c] * A0 + X[c] * as;
-      }
+      face_expand<ATT>(g, f, c0.x + c0.y, c1.x + c1.y, c2.x + c2.y, rq, sig_an);
     }
     // ---- memory variables, sources, receivers, stage update ------------------------
     float S[6];

@@ -52,42 +52,17 @@ __device__ __forceinline__ void volume_combine(const float* g, const float2* ar,
   }
 }
 
-// Expansion of the lifted amplitudes (A0, A1, A2) of face coefficients G4
-// into rq and the anelastic flux.
-template <bool ATT>
-__device__ __forceinline__ void lift_expand(const float4* G4, float A0, float A1, float A2, float as, float* rq,
-                                            float* sig_an) {
-  const float4 g0 = G4[0], g1 = G4[1], g2 = G4[2], g3 = G4[3], g4 = G4[4], g5 = G4[5], g6 = G4[6];
-  const float G[28] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w, g2.x, g2.y, g2.z, g2.w, g3.x, g3.y,
-                       g3.z, g3.w, g4.x, g4.y, g4.z, g4.w, g5.x, g5.y, g5.z, g5.w, g6.x, g6.y, g6.z, g6.w};
-  float X[6];
-#pragma unroll
-  for (int c = 0; c < 6; ++c) X[c] = G[6 + c] * A1 + G[12 + c] * A2;
-#pragma unroll
-  for (int c = 0; c < 6; ++c) rq[c] += G[c] * A0 + X[c];
-  rq[6] += G[18] * A0 + G[21] * A1 + G[24] * A2;
-  rq[7] += G[19] * A0 + G[22] * A1 + G[25] * A2;
-  rq[8] += G[20] * A0 + G[23] * A1 + G[26] * A2;
-  if (ATT) {
-    const float4 g7 = G4[7], g8 = G4[8];
-    const float NN[6] = {G[27], g7.x, g7.y, g7.z, g7.w, g8.x};
-#pragma unroll
-    for (int c = 0; c < 6; ++c) sig_an[c] += NN[c] * A0 + X[c] * as;
-  }
-}
-
 template <int N, bool ATT, int MODE>
 __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
   using O = Order<N, 2>;
-  constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, QS = O::QS, GS = O::GS, NPP = O::NPP;
+  constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, QS = O::QS, NPP = O::NPP;
   extern __shared__ __align__(16) float smem[];
   float* sD = smem;
   float* sL = sD + O::SD;
   float* sBuf = sL + O::SL;
   float* sQI = sBuf + 2 * O::BUF;
   float* sAmp = sQI + O::SQI;
-  float* sG = sAmp + O::SAMP;
-  unsigned char* sPat = reinterpret_cast<unsigned char*>(sG + O::SG);
+  unsigned char* sPat = reinterpret_cast<unsigned char*>(sAmp + O::SAMP);
 
   const int tid = threadIdx.x;
   for (int i = tid; i < 3 * Np * Np; i += blockDim.x) sD[i] = a.D[i];
@@ -178,8 +153,6 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
       am[O::NFP] = as1 * fs;
       am[2 * O::NFP] = as2 * fs;
     }
-    for (int i = tid; i < ne * 4; i += blockDim.x)
-      face_coeffs(sGeo + (i >> 2) * GEO_STRIDE, i & 3, sG + (i >> 2) * O::GE + (i & 3) * GS);
     __syncthreads();
     if (!active) continue;
 
@@ -225,7 +198,6 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
     float sa1[6], sa2[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) { sa1[c] = 0.f; sa2[c] = 0.f; }
-    const float as = ATT ? g[G_AS] : 0.f;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
       float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0, s0 = p0, s1 = p0, s2 = p0;
@@ -244,9 +216,8 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
         s1 = __ffma2_rn(l2, u1, s1);
         s2 = __ffma2_rn(l2, u2, s2);
       }
-      const float4* G4 = reinterpret_cast<const float4*>(sG + le * O::GE + f * GS);
-      lift_expand<ATT>(G4, p0.x + p0.y, p1.x + p1.y, p2.x + p2.y, as, rq1, sa1);
-      lift_expand<ATT>(G4, s0.x + s0.y, s1.x + s1.y, s2.x + s2.y, as, rq2, sa2);
+      face_expand<ATT>(g, f, p0.x + p0.y, p1.x + p1.y, p2.x + p2.y, rq1, sa1);
+      face_expand<ATT>(g, f, s0.x + s0.y, s1.x + s1.y, s2.x + s2.y, rq2, sa2);
     }
     // ---- memory variables, sources, receivers, stage update --------------------------
     auto strain = [&](const float* sig_an, const float* vgrad, float* S) {
