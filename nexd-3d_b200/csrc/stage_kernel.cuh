@@ -182,52 +182,16 @@ __device__ __forceinline__ bool face_jump(const StageArgs& a, int b, int code, i
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 
-// Expansion coefficients of one face (the rank-3 form of T (A+|A|) T^-1).
-__device__ __forceinline__ void face_coeffs(const float* g, int f, float* out) {
-  const float nx = g[G_N + 3 * f], ny = g[G_N + 3 * f + 1], nz = g[G_N + 3 * f + 2];
-  const float sx = g[G_S + 3 * f], sy = g[G_S + 3 * f + 1], sz = g[G_S + 3 * f + 2];
-  const float tx = g[G_T + 3 * f], ty = g[G_T + 3 * f + 1], tz = g[G_T + 3 * f + 2];
-  const float c = g[G_C];
-  // P = n n^T + c (s s^T + t t^T)   (Voigt xx yy zz xy yz xz)
-  out[0] = nx * nx + c * (sx * sx + tx * tx);
-  out[1] = ny * ny + c * (sy * sy + ty * ty);
-  out[2] = nz * nz + c * (sz * sz + tz * tz);
-  out[3] = nx * ny + c * (sx * sy + tx * ty);
-  out[4] = ny * nz + c * (sy * sz + ty * tz);
-  out[5] = nx * nz + c * (sx * sz + tx * tz);
-  // S1 = n s^T + s n^T
-  out[6] = 2.f * nx * sx;
-  out[7] = 2.f * ny * sy;
-  out[8] = 2.f * nz * sz;
-  out[9] = nx * sy + ny * sx;
-  out[10] = ny * sz + nz * sy;
-  out[11] = nx * sz + nz * sx;
-  // S2 = n t^T + t n^T
-  out[12] = 2.f * nx * tx;
-  out[13] = 2.f * ny * ty;
-  out[14] = 2.f * nz * tz;
-  out[15] = nx * ty + ny * tx;
-  out[16] = ny * tz + nz * ty;
-  out[17] = nx * tz + nz * tx;
-  const float izp = g[G_IZP], izs = g[G_IZS];
-  out[18] = -nx * izp; out[19] = -ny * izp; out[20] = -nz * izp;
-  out[21] = -sx * izs; out[22] = -sy * izs; out[23] = -sz * izs;
-  out[24] = -tx * izs; out[25] = -ty * izs; out[26] = -tz * izs;
-  // anelastic: n n^T / (lambda + 2 mu)
-  const float ap = g[G_AP];
-  out[27] = nx * nx * ap; out[28] = ny * ny * ap; out[29] = nz * nz * ap;
-  out[30] = nx * ny * ap; out[31] = ny * nz * ap; out[32] = nx * nz * ap;
-  out[33] = 0.f; out[34] = 0.f; out[35] = 0.f;
-}
-
 // Lifted upwind flux of face f expanded to the 9 fields and the anelastic
-// stress flux, from the lifted amplitudes A0 (P), A1, A2 (S along s, t).  The
-// rank-3 form A0 [n n^T + c (s s^T + t t^T)] + A1 (n s^T + s n^T) +
-// A2 (n t^T + t n^T) of face_coeffs is evaluated with s s^T + t t^T = I - n n^T
-// ((n, s, t) orthonormal) as n v^T + v n^T + c A0 I, v = (1-c)/2 A0 n + m,
-// m = A1 s + A2 t; velocity -(A0 n / Zp + m / Zs); anelastic
+// stress flux, from the lifted amplitudes A0 (P), A1, A2 (S along s, t): the
+// rank-3 form of T (A+|A|) T^-1 gives the stresses (Voigt xx yy zz xy yz xz)
+// A0 [n n^T + c (s s^T + t t^T)] + A1 (n s^T + s n^T) + A2 (n t^T + t n^T),
+// c = lambda/(lambda+2mu), evaluated with s s^T + t t^T = I - n n^T ((n, s, t)
+// orthonormal) as n v^T + v n^T + c A0 I, v = (1-c)/2 A0 n + m,
+// m = A1 s + A2 t; the velocities -(A0 n / Zp + m / Zs); the anelastic flux
 // A0 n n^T / (lambda+2mu) + (n m^T + m n^T) / (2 mu) = n u^T + u n^T.
-// Reads 9 words of the element record per face instead of 36 coefficients.
+// Reads 9 words of the element record per face and accumulates into rq and
+// sig_an.
 template <bool ATT>
 __device__ __forceinline__ void face_expand(const float* g, int f, float A0, float A1, float A2, float* rq,
                                             float* sig_an) {

@@ -213,22 +213,11 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
       face_amplitudes(g, f, dq, free_face, ap, as1, as2);
       const float fs = g[G_FS + f];
       const float a0 = ap * fs, a1 = as1 * fs, a2 = as2 * fs;
-      float cf[36];
-      face_coeffs(g, f, cf);
+      // the face flux of this face node: 9 fields, then the anelastic flux (zero when elastic)
       float v[16];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) v[c] = cf[c] * a0 + (cf[6 + c] * a1 + cf[12 + c] * a2);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) v[6 + c] = cf[18 + c] * a0 + cf[21 + c] * a1 + cf[24 + c] * a2;
-      if (ATT) {
-        const float as = g[G_AS];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) v[9 + c] = cf[27 + c] * a0 + (cf[6 + c] * a1 + cf[12 + c] * a2) * as;
-      } else {
-#pragma unroll
-        for (int c = 9; c < 15; ++c) v[c] = 0.f;
-      }
-      v[15] = 0.f;
+      for (int c = 0; c < 16; ++c) v[c] = 0.f;
+      face_expand<ATT>(g, f, a0, a1, a2, v, v + 9);
       tc::store_a16x3(sA, T::A_BYTES, ee * T::COLS, T::KV16 + j, v, T::A_LBO, T::A_SBO);
     }
     tc::fence_async_smem();
