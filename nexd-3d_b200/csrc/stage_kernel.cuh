@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
 #pragma unroll
       for (int j = 0; j < 4; ++j) { ar[j] = make_float2(0.f, 0.f); as_[j] = ar[j]; at[j] = ar[j]; }
       const float* qe = sQI + le * O::QE;
-#pragma unroll 5
+#pragma unroll
       for (int k = 0; k < Np; ++k) {
         const float dx = sD[k * Np + n], dy = sD[Np * Np + k * Np + n], dz = sD[2 * Np * Np + k * Np + n];
         const float2 d0 = make_float2(dx, dx), d1 = make_float2(dy, dy), d2 = make_float2(dz, dz);
@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       float v2r = 0.f, v2s = 0.f, v2t = 0.f;
       const float* cfe = sCF + le * O::CFE;
       const float* qv = sQF + le * Np;
-#pragma unroll 2
+#pragma unroll 5
       for (int k = 0; k < Np; ++k) {
         const float4 d = make_float4(sD[k * Np + n], sD[Np * Np + k * Np + n], sD[2 * Np * Np + k * Np + n], 0.f);
         const float2 d0 = make_float2(d.x, d.x), d1 = make_float2(d.y, d.y), d2 = make_float2(d.z, d.z);
