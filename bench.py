@@ -67,7 +67,7 @@ WORKLOADS = {
 }
 
 
-def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.5):
+def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.5, epochs=30):
     """Learned boundary at training scale: 2 x 2 x 1 km two-layer models (1,536
     tets) with seeded random layers (vp 2500-5500 m/s, vp/vs 1.6-1.9, rho
     2200-2900 kg/m^3) inside an 8-element NPML; train the boundary MLP on
@@ -86,7 +86,7 @@ def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.
     x, y = np.concatenate(xs), np.concatenate(ys)
     t_data = time.perf_counter() - t0
     tr = boundary.Trainer(9 * 15, batch=2048, lr=1e-3, seed=0)
-    hist = tr.fit(x, y, epochs=30)
+    hist = tr.fit(x, y, epochs=epochs)
     t_train = time.perf_counter() - t0 - t_data
     params = tr.parameters()
     scores = []
@@ -95,7 +95,7 @@ def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.
         scores.append(res)
     mean = lambda k, f: float(np.mean([np.mean(r[k][f]) for r in scores]))
     summary = {"train_sources": n_train, "heldout_sources": n_eval, "materials": "seeded random two-layer",
-               "samples": int(len(x)),
+               "samples": int(len(x)), "epochs": epochs,
                "loss_first_last": [hist[0], hist[-1]], "data_s": round(t_data, 1), "train_s": round(t_train, 1),
                "max_reflection": max_reflection,
                "field_err_vs_wide_npml": {"plain": mean("plain", "field_err"), "learned": mean("learned", "field_err")},
@@ -292,6 +292,9 @@ def main():
                          "(the choice an auto run reports in kernels_per_class; profiled runs use it, since "
                          "timing under a profiler would change the auto choice)")
     ap.add_argument("--workload", default="twolayer", choices=sorted(WORKLOADS))
+    ap.add_argument("--lb-train", type=int, default=16, help="learned workload: training source/material pairs")
+    ap.add_argument("--lb-eval", type=int, default=4, help="learned workload: held-out pairs scored")
+    ap.add_argument("--lb-epochs", type=int, default=30, help="learned workload: training epochs")
     ap.add_argument("--cells", default=None, help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
     args = ap.parse_args()
     grp = replicas.init()
@@ -331,7 +334,8 @@ def main():
             torch.cuda.set_device(0)
         learned = None
         if args.workload == "learned":
-            lb_params, learned = train_learned_boundary(tmp)
+            lb_params, learned = train_learned_boundary(tmp, n_train=args.lb_train, n_eval=args.lb_eval,
+                                                        epochs=args.lb_epochs)
         d = os.path.join(tmp, "model")
         if args.workload == "cube":
             synth.write_cube(d, cells=cells[0], nt=wl["nt"], seed=replicas.replica_seed(1, rank))
