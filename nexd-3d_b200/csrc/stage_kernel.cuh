@@ -645,9 +645,14 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     }
     // ---- interleaved own wavefield for the volume loop ------------------------------
     if (!PML && active) {
+      // two 16-byte stores and one 4-byte store: a 16-byte store of 8 threads
+      // at a 12-word stride touches 32 different banks
       float* dst = sQI + le * O::QE + n * QS;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) dst[c] = sQF[c * (E * Np) + le * Np + n];
+      const float* src = sQF + le * Np + n;
+      constexpr int FS = E * Np;
+      *reinterpret_cast<float4*>(dst) = make_float4(src[0], src[FS], src[2 * FS], src[3 * FS]);
+      *reinterpret_cast<float4*>(dst + 4) = make_float4(src[4 * FS], src[5 * FS], src[6 * FS], src[7 * FS]);
+      dst[8] = src[8 * FS];
     }
     // ---- face amplitudes and expansion coefficients -----------------------------
     for (int i = tid; i < ne * NF; i += blockDim.x) {
@@ -806,12 +811,21 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       float2 c0 = make_float2(0.f, 0.f), c1 = c0, c2 = c0;
       const float2* lp = reinterpret_cast<const float2*>(sL) + f * O::NPAIR * Np + n;
       const float* ax = sAmp + le * O::AE + f * 2 * O::NPAIR;
+      // face-node pairs; with NpF odd the last face node alone (its pair's
+      // second slot is zero padding), as 4-byte loads
+      constexpr int FULL = NpF / 2;
 #pragma unroll
-      for (int ip = 0; ip < O::NPAIR; ++ip) {
+      for (int ip = 0; ip < FULL; ++ip) {
         const float2 l = lp[ip * Np];
         c0 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + 2 * ip), c0);
         c1 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + O::NFP + 2 * ip), c1);
         c2 = __ffma2_rn(l, *reinterpret_cast<const float2*>(ax + 2 * O::NFP + 2 * ip), c2);
+      }
+      if constexpr (NpF & 1) {
+        const float l = reinterpret_cast<const float*>(lp + FULL * Np)[0];
+        c0.x = fmaf(l, ax[2 * FULL], c0.x);
+        c1.x = fmaf(l, ax[O::NFP + 2 * FULL], c1.x);
+        c2.x = fmaf(l, ax[2 * O::NFP + 2 * FULL], c2.x);
       }
       face_expand<ATT>(g, f, c0.x + c0.y, c1.x + c1.y, c2.x + c2.y, rq, sig_an);
     }
