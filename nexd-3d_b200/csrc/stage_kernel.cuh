@@ -22,8 +22,9 @@
 //    Np x Np matvecs) and applies the element-constant metric and material;
 //  * the upwind flux T (A+|A|) T^-1 has rank 3 (one P and two S
 //    characteristics), so each face node contributes three amplitudes; LIFT is
-//    applied to the amplitudes and expanded with per-face 9x3 coefficients,
-//    and the same lifted amplitudes give the anelastic flux;
+//    applied to the amplitudes, which are expanded to the 9 fields from the
+//    face frame (n, s, t), and the same lifted amplitudes give the anelastic
+//    flux;
 //  * NPML elements (grouped first in the internal element order) are handled
 //    by the PML instantiation, which differentiates the 27 modified flux
 //    columns through their contravariant components (Dr Fr + Ds Fs + Dt Ft).
@@ -45,7 +46,6 @@ struct Order {
   static constexpr int NPP = (Np + NPT - 1) / NPT;    // threads per element
   static constexpr int E = NPT * (THREADS / Np);     // elements per chunk
   static constexpr int QS = 12;           // padded field stride of staged q (3 x float4)
-  static constexpr int GS = 36;           // per-face expansion coefficients
   static constexpr int CS = 34;           // contravariant-flux row stride (PML): r 0..9, s 10..19, t 20..29
   // shared-memory section sizes in floats, each a multiple of 4 (float4 alignment)
   static constexpr int r4(int x) { return (x + 3) / 4 * 4; }
@@ -684,12 +684,22 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       float F[9], G[9], H[9];
       elastic_fluxes(g, qv, F, G, H);
       pml_node<ATT, MODE>(a, b, node, pf, F, G, H);
-      float* cf = sCF + le * O::CFE + n * CS;
+      // the row as 8-byte stores (pairs of fields; field 8 with the zero pad):
+      // 16 threads at a 34-word stride touch 32 different banks
+      float2* cf = reinterpret_cast<float2*>(sCF + le * O::CFE + n * CS);
+      float r[10], sv[10], t[10];
 #pragma unroll
       for (int i = 0; i < 9; ++i) {
-        cf[i] = g[G_RX] * F[i] + g[G_RY] * G[i] + g[G_RZ] * H[i];
-        cf[10 + i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
-        cf[20 + i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
+        r[i] = g[G_RX] * F[i] + g[G_RY] * G[i] + g[G_RZ] * H[i];
+        sv[i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
+        t[i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
+      }
+      r[9] = sv[9] = t[9] = 0.f;
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        cf[j] = make_float2(r[2 * j], r[2 * j + 1]);
+        cf[5 + j] = make_float2(sv[2 * j], sv[2 * j + 1]);
+        cf[10 + j] = make_float2(t[2 * j], t[2 * j + 1]);
       }
     }
     __syncthreads();
