@@ -654,7 +654,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       *reinterpret_cast<float4*>(dst + 4) = make_float4(src[4 * FS], src[5 * FS], src[6 * FS], src[7 * FS]);
       dst[8] = src[8 * FS];
     }
-    // ---- face amplitudes and expansion coefficients -----------------------------
+    // ---- face amplitudes ---------------------------------------------------------
     for (int i = tid; i < ne * NF; i += blockDim.x) {
       const int ee = i / NF, j = i - ee * NF;
       const int f = j / NpF, fi = j - f * NpF;
