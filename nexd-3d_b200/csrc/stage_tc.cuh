@@ -240,13 +240,16 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
       break;
     }
     tc::fence_after_sync();
-    if (warp < 4) {
-      // lane m holds row m: node columns n of the h, m, l blocks at n, NP16 + n, 2 NP16 + n
-      const int m = 32 * warp + (tid & 31);
-      const uint32_t ta = tmem + (uint32_t(32 * warp) << 16);
+    {
+      // lane m holds row m: node columns n of the h, m, l blocks at n, NP16 + n, 2 NP16 + n;
+      // warp w reads TMEM lanes 32 (w % 4) .. +31, warps 0-3 the column groups
+      // 0, 64, ..., warps 4-7 the groups 32, 96, ...
+      const int quarter = warp & 3;
+      const int m = 32 * quarter + (tid & 31);
+      const uint32_t ta = tmem + (uint32_t(32 * quarter) << 16);
       float* r = sR + m * T::RS;
 #pragma unroll
-      for (int c0 = 0; c0 < T::NP16; c0 += 32) {
+      for (int c0 = 32 * (warp >> 2); c0 < T::NP16; c0 += 64) {
         constexpr int W32 = 32;
         float v0[W32], v1[W32], v2[W32];
         const bool wide = T::NP16 - c0 >= 32;
