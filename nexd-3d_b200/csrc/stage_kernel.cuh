@@ -55,7 +55,11 @@ struct Order {
   static constexpr int SL = 4 * NPAIR * Np * 2; // LIFT as [face][pair][n][2]
   // one prefetch buffer: element records, own wavefield (field-major), the
   // neighbour face traces and the connectivity of the following chunk
-  static constexpr int SGEO = E * 64;
+  // element records at a 68-word stride: the same field of different
+  // elements in one warp falls on different banks (a 64-word stride puts it
+  // on one bank)
+  static constexpr int GSTR = 68;
+  static constexpr int SGEO = E * GSTR;
   static constexpr int SQF = r4(9 * E * Np);
   static constexpr int STR = r4(E * NF * 9);
   static constexpr int SIDS = r4(E * 12);
@@ -287,7 +291,8 @@ __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, f
   constexpr int Np = O::Np, E = O::E;
   const int tid = threadIdx.x, nth = blockDim.x;
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
-  for (int i = tid; i < c.ne * 16; i += nth) cp_async16(bGeo + 4 * i, a.geo + (long long)c.e0 * GEO_STRIDE + 4 * i);
+  for (int i = tid; i < c.ne * 16; i += nth)
+    cp_async16(bGeo + (i >> 4) * O::GSTR + 4 * (i & 15), a.geo + (long long)c.e0 * GEO_STRIDE + 4 * i);
   const int cnt = c.ne * Np;
   const long long base = (long long)c.e0 * Np;
   for (int i = tid; i < 9 * E * Np; i += nth) {
@@ -658,7 +663,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     for (int i = tid; i < ne * NF; i += blockDim.x) {
       const int ee = i / NF, j = i - ee * NF;
       const int f = j / NpF, fi = j - f * NpF;
-      const float* g = sGeo + ee * GEO_STRIDE;
+      const float* g = sGeo + ee * O::GSTR;
       const int code = sIds[ee * 12 + 8 + f];
       const int own = sPat[f * NpF + fi];  // patterns 0..3 are the element's own face masks
       const float* qo = sQF + ee * Np + own;
@@ -677,7 +682,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     float vgrad[9];  // d(v_c)/d(x_d) [c*3+d] (anelastic)
     (void)vgrad;
     if constexpr (PML) if (active) {
-      const float* g = sGeo + le * GEO_STRIDE;
+      const float* g = sGeo + le * O::GSTR;
       float qv[9];
 #pragma unroll
       for (int c = 0; c < 9; ++c) qv[c] = sQF[c * (E * Np) + le * Np + n];
@@ -706,7 +711,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     if (!active) continue;  // idle threads of a partial chunk (the next barrier is at the loop top)
 
     const int e = e0 + le;
-    const float* g = sGeo + le * GEO_STRIDE;
+    const float* g = sGeo + le * O::GSTR;
     float rq[9];
     // ---- volume term ------------------------------------------------------------
     if (!PML) {

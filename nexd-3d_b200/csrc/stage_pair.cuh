@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
     for (int i = tid; i < ne * NF; i += blockDim.x) {
       const int ee = i / NF, j = i - ee * NF;
       const int f = j / NpF, fi = j - f * NpF;
-      const float* g = sGeo + ee * GEO_STRIDE;
+      const float* g = sGeo + ee * O::GSTR;
       const int code = sIds[ee * 12 + 8 + f];
       const int own = sPat[f * NpF + fi];
       const float* qo = sQF + ee * Np + own;
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
     if (!active) continue;
 
     const int e = e0 + le;
-    const float* g = sGeo + le * GEO_STRIDE;
+    const float* g = sGeo + le * O::GSTR;
     float rq1[9], rq2[9], vg1[9], vg2[9];
     (void)vg1;
     (void)vg2;

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
 
     // ---- volume fluxes: data rows K = d Np + node ------------------------------
     if (active) {
-      const float* g = sGeo + le * GEO_STRIDE;
+      const float* g = sGeo + le * O::GSTR;
       float qv[9];
 #pragma unroll
       for (int c = 0; c < 9; ++c) qv[c] = sQF[c * (E * Np) + le * Np + n];
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
     for (int i = tid; i < ne * NF; i += blockDim.x) {
       const int ee = i / NF, j = i - ee * NF;
       const int f = j / NpF, fi = j - f * NpF;
-      const float* g = sGeo + ee * GEO_STRIDE;
+      const float* g = sGeo + ee * O::GSTR;
       const int code = sIds[ee * 12 + 8 + f];
       const int own = sPat[f * NpF + fi];
       const float* qo = sQF + ee * Np + own;
