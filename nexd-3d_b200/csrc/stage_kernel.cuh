@@ -778,9 +778,10 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     } else {
 #pragma unroll
       for (int c = 0; c < 9; ++c) rq[c] = 0.f;
-      float2 acc[5];
+      float2 acc[4];  // fields 0..7 in pairs; field 8 as 4-byte loads (its pair's second word is padding)
+      float acc8 = 0.f;
 #pragma unroll
-      for (int j = 0; j < 5; ++j) acc[j] = make_float2(0.f, 0.f);
+      for (int j = 0; j < 4; ++j) acc[j] = make_float2(0.f, 0.f);
       float2 v01r = make_float2(0.f, 0.f), v01s = v01r, v01t = v01r;
       float v2r = 0.f, v2s = 0.f, v2t = 0.f;
       const float* cfe = sCF + le * O::CFE;
@@ -791,7 +792,9 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
         const float2 d0 = make_float2(d.x, d.x), d1 = make_float2(d.y, d.y), d2 = make_float2(d.z, d.z);
         const float2* cf = reinterpret_cast<const float2*>(cfe + k * CS);
 #pragma unroll
-        for (int j = 0; j < 5; ++j) acc[j] = __ffma2_rn(d0, cf[j], __ffma2_rn(d1, cf[5 + j], __ffma2_rn(d2, cf[10 + j], acc[j])));
+        for (int j = 0; j < 4; ++j) acc[j] = __ffma2_rn(d0, cf[j], __ffma2_rn(d1, cf[5 + j], __ffma2_rn(d2, cf[10 + j], acc[j])));
+        const float* c8 = cfe + k * CS + 8;
+        acc8 = fmaf(d.x, c8[0], fmaf(d.y, c8[10], fmaf(d.z, c8[20], acc8)));
         if (ATT) {
           const float2 v01 = make_float2(qv[6 * (E * Np) + k], qv[7 * (E * Np) + k]);
           const float v2 = qv[8 * (E * Np) + k];
@@ -805,7 +808,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) { rq[2 * j] = acc[j].x; rq[2 * j + 1] = acc[j].y; }
-      rq[8] = acc[4].x;
+      rq[8] = acc8;
       const float vr[3] = {v01r.x, v01r.y, v2r}, vs3[3] = {v01s.x, v01s.y, v2s}, vt3[3] = {v01t.x, v01t.y, v2t};
       if (ATT) {
 #pragma unroll
