@@ -193,3 +193,20 @@ def test_database_errors(tmp_path):
     _corrupt(mv, off + 4, dr.astype("<f4").tobytes())
     with pytest.raises(NexdError, match="do not match"):
         Mesh(d, database=True)
+
+
+@pytest.mark.parametrize("N", [2, 3, 5])
+def test_round_trip_other_orders(tmp_path, N):
+    """The reader takes the order from the records: elastic cube at N = 2, 3,
+    5 written and read back gives the mesher's descriptor."""
+    d = str(tmp_path / f"cube{N}")
+    synth.write_cube(d, cells=2, nt=6)
+    m = Mesh(d, N=N)
+    m.write_database(os.path.join(d, "out"))
+    m2 = Mesh(d, N=4, database=True)  # the order argument is ignored
+    assert (m2.N, m2.Np, m2.NpF, m2.K) == (m.N, m.Np, m.NpF, m.K)
+    for name in ("neighbor", "face", "ibn", "fmask", "srcelem", "recelem"):
+        assert np.array_equal(m2.array(name), m.array(name)), name
+    for name in ("metric", "fscale", "nnormal", "Dr", "lift", "srcInt", "recInt"):
+        a, b = m.array(name), m2.array(name)
+        assert np.abs(a - b).max() <= 4e-7 * np.abs(a).max(), name
