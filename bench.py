@@ -194,9 +194,9 @@ def run_multimodel(args, grp, tmp, steps, warmup):
     for s in solvers:
         s.close()
 N_ORDER = 4
-# CPU sample: same model family and order at 20x20x10 cells (24,000 tets)
-CPU_SAMPLE_CELLS = (20, 20, 10)
-CPU_SAMPLE_STEPS = 6
+# CPU baseline: a bounded number of steps of the timed model itself (the same
+# mesh), the time of the oracle's step loop only (set-up excluded)
+CPU_STEPS = 2
 
 
 def load_peaks():
@@ -250,30 +250,43 @@ def summarize_clocks(path, device):
             "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def oracle_baseline(tmp, workload="twolayer", steps=CPU_SAMPLE_STEPS):
-    """FP32 CPU restatement of the reference solver on a bounded sample."""
+def oracle_baseline(tmp, workload="twolayer", mesh=None, steps=CPU_STEPS, seed=None):
+    """The CPU restatement of the reference solver (the oracle, FP32 like the
+    reference's default CUSTOM_REAL) on the host cores, all OpenMP threads,
+    over `steps` steps of the same workload (the mesh given, or one built
+    with the same generator, sizes and seed); the rate counts the step loop
+    only.  Returns (DOF-stage/s, threads, sample description)."""
     lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
     lib.oracle_run.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_void_p, C.c_int]
-    d = os.path.join(tmp, "cpu_sample")
+    lib.oracle_loop_seconds.restype = C.c_double
+    if WORKLOADS[workload]["cells"] is None:  # the multi-model group: its largest member family
+        workload = "twolayer"
+    if mesh is None:
+        d = os.path.join(tmp, "cpu_model")
+        wl = WORKLOADS[workload]
+        seed = replicas.replica_seed(1 if workload == "cube" else 2, 0) if seed is None else seed
+        if workload == "cube":
+            synth.write_cube(d, cells=wl["cells"][0], nt=wl["nt"], seed=seed)
+        else:
+            nsrc = wl.get("nsrc", 1)
+            kw = dict(src_depth=(500.0, 1800.0), f0_range=(2.0, 4.0)) if nsrc > 1 else {}
+            synth.write_twolayer(d, cells=wl["cells"], nt=wl["nt"], nrec=100, nsrc=nsrc, src_seed=seed,
+                                 pml=(workload != "learned"), **kw)
+        mesh = Mesh(d, N=wl["N"], stf_stage_time=True, nbatch=wl.get("nsrc", 1))
+    m = mesh
     if workload == "cube":
-        steps = 60
-        synth.write_cube(d, nt=steps)
-        m = Mesh(d, N=3, stf_stage_time=True)
-        what = f"{steps} LSERK4 steps of the full cube ({m.K} tets, N=3, elastic, absorbing)"
-    else:
-        synth.write_twolayer(d, cells=CPU_SAMPLE_CELLS, nt=steps)
-        m = Mesh(d, N=N_ORDER, stf_stage_time=True)
-        what = (f"{steps} LSERK4 steps of the same model family at {CPU_SAMPLE_CELLS[0]}x{CPU_SAMPLE_CELLS[1]}x"
-                f"{CPU_SAMPLE_CELLS[2]} cells ({m.K} tets, N={N_ORDER}, anelastic + NPML, one source)")
+        steps = max(steps, 20)
     tr = np.zeros((m.nrec, m.nt, 9, m.nbatch), dtype=np.float32, order="F")
     t0 = time.perf_counter()
     st = lib.oracle_run(m.desc_ptr, 32, steps, tr.ctypes.data_as(C.POINTER(C.c_float)), None, 0)
-    el = time.perf_counter() - t0
+    wall = time.perf_counter() - t0
     if st != 0:
         raise RuntimeError(f"oracle failed: {st}")
-    units = 9 * m.Np * m.K * 5 * steps
+    el = lib.oracle_loop_seconds()
+    units = 9 * m.Np * m.K * 5 * steps * m.nbatch
     cores = os.cpu_count() or 1
-    sample = f"{what}, FP32, {cores} OpenMP threads, {el:.1f} s"
+    sample = (f"{steps} LSERK4 steps of the timed workload itself ({m.K} tets, N={m.N}, {m.nbatch} wavefield(s)), "
+              f"FP32, {cores} OpenMP threads; step loop {el:.1f} s (set-up excluded, {wall:.1f} s wall in total)")
     return units / el, cores, sample
 
 
@@ -318,11 +331,14 @@ def main():
     try:
         if args.impl == "reference":
             if rank == 0:
-                v, cores, sample = oracle_baseline(tmp, args.workload)
+                v, cores, sample = oracle_baseline(tmp, args.workload, steps=CPU_STEPS)
                 line = {"metric": metric, "value": v, "unit": "DOF-stage/s", "n_gpus": args.gpus, "steps": steps,
                         "warmup": warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
                         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                        "config": {"workload": workload, "sample": "see cpu_baseline"}, "impl": "reference",
+                        "config": {"workload": workload, "tets": wl["cells"][0] * wl["cells"][1] * wl["cells"][2] * 6
+                                   if wl["cells"] else None, "N": wl["N"], "integrator": "LSERK4 (5 stages)",
+                                   "sample": f"{CPU_STEPS} steps of this workload (see cpu_baseline)"},
+                        "impl": "reference",
                         "cpu_baseline": {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port",
                                          "sample": sample},
                         "e2e": {"value": v, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -357,9 +373,9 @@ def main():
         if learned is not None:
             s.set_boundary_mlp(lb_params, learned["max_reflection"])
         nstage = 5
-        need = warmup + 3 * steps
+        need = warmup + 3 * steps + 1
         if need > mesh.nt:
-            raise SystemExit(f"--warmup + 3*--steps must be <= {mesh.nt}")
+            raise SystemExit(f"--warmup + 3*--steps + 1 must be <= {mesh.nt}")
         s.run(1, warmup)
         grp.barrier()
         torch.cuda.synchronize()
@@ -393,14 +409,20 @@ def main():
         stf_all = mesh.array("stf")  # (nspt, nt, nsrc)
         stf_in = np.zeros((nspt, nsrc), dtype=np.float32, order="F")
         tr_out = np.zeros((nrec, 9, mesh.nbatch), dtype=np.float32, order="F")
+        # one untimed streaming step first: it captures the one-step graphs
+        it_first = warmup + 2 * steps + 1
+        stf_in[:, :] = stf_all[:, it_first - 1, :]
+        s.step_io(it_first, stf_in, tr_out)
         grp.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for it in range(warmup + 2 * steps + 1, warmup + 3 * steps + 1):
+        for it in range(it_first + 1, it_first + steps + 1):
             stf_in[:, :] = stf_all[:, it - 1, :]
             s.step_io(it, stf_in, tr_out)
         e2e_s = grp.max(time.perf_counter() - t0)
         e2e = total_units / e2e_s
+        # end of run: every replica's receiver traces on rank 0 (outside the timed regions)
+        gathered = replicas.gather_traces(grp, s.traces())
         if rank != 0:
             return
         peak, peak_kind = load_peaks()
@@ -411,17 +433,19 @@ def main():
         abytes = algorithmic_bytes(mesh, dom, prof[dom]["elements"]) * nb
         achieved = abytes / (per_launch_ms * 1e-3) / 1e9
         traffic = None
+        ckinds = s.contraction()[0]
         tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
         if os.path.exists(tp):
             try:
-                kind = s.contraction()[0]["npml" if dom == "stage_pml" else "rest"]
+                kind = ckinds["npml" if dom == "stage_pml" else "rest"]
                 t = json.load(open(tp)).get(workload, {}).get(f"{dom}/{kind}")
                 traffic = None if t is None else float(t)
             except Exception:
                 traffic = None
+        s.close()  # frees the device state before the CPU leg
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            v, cores, sample = oracle_baseline(tmp, args.workload)
+            v, cores, sample = oracle_baseline(tmp, args.workload, mesh=mesh)
             cpu = {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
         clocks = summarize_clocks(clk_file, local) if clk else None
         state_gb = (2 * 9 + 9 + 2 * 6 * mesh.desc.nMB) * mesh.K * mesh.Np * 4 * nb / 1e9
@@ -429,13 +453,13 @@ def main():
             "metric": metric, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32" if set(s.contraction()[0].values()) == {"fp32"} else
+            "dtype": "f32" if set(ckinds.values()) == {"fp32"} else
                      "f32 state and update; contraction as three-way split bf16 on tcgen05 with f32 accumulation",
             "data": "synthetic (seeded two-layer model, per-rank seeded source)",
             "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
                        "integrator": "LSERK4 (5 stages)",
                        "contraction": contraction,
-                       "kernels_per_class": s.contraction()[0], "pml_tets": int(prof["stage_pml"]["elements"]),
+                       "kernels_per_class": ckinds, "pml_tets": int(prof["stage_pml"]["elements"]),
                        "receivers": nrec, "sources_per_rank": nsrc, "wavefields_per_rank": nb,
                        "timed": "CUDA graphs of two steps; roofline from a per-launch-event pass of K more steps",
                        "l2": f"inputs larger than L2: {state_gb:.1f} GB of state streamed per stage",
@@ -451,12 +475,12 @@ def main():
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "traces_gathered_on_rank0": list(gathered.shape),
         }
         if learned is not None:
             line["learned_boundary"] = learned
             line["kernels"]["boundary"] = {"launches": prof["boundary"]["launches"], "ms": round(prof["boundary"]["ms"], 3)}
         print(json.dumps(line), flush=True)
-        s.close()
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
         grp.close()

@@ -199,14 +199,18 @@ int nexd_get_energy(nexd_ctx* ctx, double* energy, int32_t* pml_switch);
  *
  * Same computation as the trigger's energy (nexd_pml_trigger, formula 0 or 1);
  * the block partial sums go to a fixed scratch array inside libnexd.so
- * (NEXD_NOALLOC_MAX_BATCH wavefields x 256 blocks of FP64, 128 KiB), held by
- * every GPU that loads the library until the process exits.
+ * (NEXD_NOALLOC_MAX_BATCH wavefields x 256 blocks of FP64 plus one total per
+ * wavefield: 16,448 doubles = 128.5 KiB), held by every GPU that loads the
+ * library until the process exits.
  *   q:      device, field-major (nelem*Np nodes per field), field stride ldq,
- *           wavefield stride 9*ldq
- *   emat:   device, (4, nelem) FP32: rho, lambda, mu, J per element
- *   mass:   device, (Np, Np) FP64 mass matrix
- *   energy: host, nbatch FP64 results
- * nbatch above NEXD_NOALLOC_MAX_BATCH is rejected with NEXD_ERR_INVALID.  The
+ *           wavefield stride 9*ldq; 4-byte aligned
+ *   emat:   device, (4, nelem) FP32: rho, lambda, mu, J per element; read as
+ *           16-byte vectors, so it must be 16-byte aligned
+ *   mass:   device, (Np, Np) FP64 mass matrix; 8-byte aligned
+ *   energy: host, nbatch FP64 results; 8-byte aligned
+ * A misaligned pointer is rejected with NEXD_ERR_INVALID before anything is
+ * launched.  nbatch above NEXD_NOALLOC_MAX_BATCH is rejected with
+ * NEXD_ERR_INVALID.  The
  * first call on a device looks up the scratch array's device address for that
  * device (cudaGetSymbolAddress); make that first call before any stream
  * capture.  Calls share the scratch array and leave their partial sums in it;

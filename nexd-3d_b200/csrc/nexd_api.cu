@@ -58,6 +58,7 @@ struct nexd_ctx {
   size_t smem_pml = 0, smem_main = 0;
   // device arrays
   float *D = nullptr, *L = nullptr, *geo = nullptr, *ael = nullptr, *wl = nullptr, *prof_dev = nullptr;
+  float wl_host[3] = {0.f, 0.f, 0.f};  // relaxation frequencies (kernel parameters)
   int4 *nbr = nullptr, *fcode = nullptr;
   unsigned char* patterns = nullptr;
   float* qbuf[3] = {nullptr, nullptr, nullptr};
@@ -96,6 +97,10 @@ struct nexd_ctx {
   // step counter on the device and two-step CUDA graphs (one per starting buffer parity)
   int* it_dev = nullptr;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  // one-step graphs per starting buffer (0..2) and the buffer each leaves current
+  cudaGraphExec_t gexec1[3] = {nullptr, nullptr, nullptr};
+  int gend1[3] = {0, 0, 0};
+  int graph1_launches[3] = {0, 0, 0};
   int graph_launches = 0;      // kernels per captured two-step graph
   bool graph_energy = false;   // energy_on when the graphs were captured
   bool use_graphs = true;
@@ -349,6 +354,10 @@ int validate(const nexd_desc* d) {
   }
   for (int i = 0; i < d->nrec; ++i)
     if (d->recelem[i] < 1 || d->recelem[i] > d->nelem) return set_err(nullptr, NEXD_ERR_INVALID, "recelem out of range");
+  // face masks index the element's own nodes (they become the byte-sized
+  // face patterns of the stage kernels)
+  for (int i = 0; i < 4 * NpF; ++i)
+    if (d->fmask[i] < 1 || d->fmask[i] > Np) return set_err(nullptr, NEXD_ERR_INVALID, "fmask entry out of 1..Np");
   for (int e = 0; e < d->nelem; ++e) {
     for (int f = 0; f < 4; ++f) {
       const int nb = d->neighbor[4 * e + f], fc = d->face[4 * e + f];
@@ -356,6 +365,12 @@ int validate(const nexd_desc* d) {
       if (nb == 0 && fc != -1 && fc != -2)
         return set_err(nullptr, NEXD_ERR_INVALID, "boundary face that is neither free (-1) nor absorbing (-2)");
       if (nb > 0 && (fc < 1 || fc > 4)) return set_err(nullptr, NEXD_ERR_INVALID, "interior face without neighbour face id");
+      if (nb > 0)
+        for (int i = 0; i < NpF; ++i) {
+          // ibn is a global 1-based node id that must lie inside the neighbour
+          const long long gn = (long long)d->ibn[(size_t(e) * 4 + f) * NpF + i] - 1 - (long long)(nb - 1) * Np;
+          if (gn < 0 || gn >= Np) return set_err(nullptr, NEXD_ERR_INVALID, "ibn does not point into the neighbour element");
+        }
     }
     if (!(std::fabs(d->jacobian[e]) > 0.0)) return set_err(nullptr, NEXD_ERR_INVALID, "zero Jacobian");
     if (!(d->rho[e] > 0.0) || !(d->vpu[e] > 0.0) || !(d->vsu[e] > 0.0))
@@ -544,6 +559,7 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
       }
     }
     for (int l = 0; l < c->nMB; ++l) h_wl.push_back(float(d->wl[l]));
+    for (int l = 0; l < c->nMB && l < kNMB; ++l) c->wl_host[l] = h_wl[l];
   }
   std::vector<float> h_prof;
   if (c->pml && c->Kpml > 0) {
@@ -602,6 +618,15 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   c->ldt = c->ldq;
   c->lda = ((long long)c->Kpml * Np + 63) / 64 * 64;
   const int nb = c->nbatch;
+  // per-element scalars of the stage tail in the record: Zener coefficients,
+  // first source, receiver slot (read from shared memory with the record)
+  for (int ni = 0; ni < K; ++ni) {
+    float* g = &h_geo[size_t(ni) * GEO_STRIDE];
+    if (c->att)
+      for (int j = 0; j < 3 * c->nMB; ++j) g[G_AEL + j] = h_ael[size_t(ni) * 3 * c->nMB + j];
+    std::memcpy(&g[G_SRC], &h_head[ni], sizeof(float));
+    std::memcpy(&g[G_SLOT], &h_recslot_el[ni], sizeof(float));
+  }
   if ((st = upload(c, &c->D, h_D)) || (st = upload(c, &c->L, h_L)) || (st = upload(c, &c->geo, h_geo)) ||
       (st = upload(c, &c->patterns, pat)))
     return fail(st);
@@ -725,6 +750,14 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     if ((st = upload(c, &c->ops_tc, ops4))) return fail(st);
   }
   if ((st = configure_launch(c))) return fail(st);
+  // pinned staging of nexd_step_io: (stf_per_step, nsrc) samples in, (nrec,
+  // 9, nbatch) samples out; allocated here so that no streaming step pays for it
+  c->pinned_floats = std::max<size_t>(1, size_t(c->nspt) * c->nsrc + size_t(c->nrec) * 9 * c->nbatch);
+  if (cudaMallocHost(&c->pinned, c->pinned_floats * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    c->pinned = nullptr;
+    return fail(set_err(c, NEXD_ERR_NOMEM, "pinned staging buffer for nexd_step_io"));
+  }
   CUDA_TRY(c, cudaDeviceSynchronize());
   *out = c;
   return NEXD_OK;
@@ -844,6 +877,7 @@ StageArgs base_args(nexd_ctx* c) {
   a.npat = c->npat;
   a.ael = c->ael;
   a.wl = c->wl;
+  for (int l = 0; l < kNMB; ++l) a.wlv[l] = c->att && l < c->nMB ? c->wl_host[l] : 0.f;
   a.prof = c->prof_dev;
   a.res = c->res;
   a.th = c->th;
@@ -1008,16 +1042,40 @@ void drop_graphs(nexd_ctx* c) {
       cudaGraphExecDestroy(g);
       g = nullptr;
     }
+  for (auto& g : c->gexec1)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// Captures `nsteps` steps starting from the current buffer into *exec and
+// counts its kernels; the host-side buffer index advances as the steps do.
+int capture_steps(nexd_ctx* c, int nsteps, cudaGraphExec_t* exec, int* nlaunch) {
+  const int64_t before = c->launches;
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_body(c, nsteps);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  *nlaunch = int(c->launches - before);  // kernels in the captured graph
+  c->launches = before;                  // counted when the graph runs
+  if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return NEXD_OK;
 }
 
 // Enqueues steps it_begin..it_end: pairs of steps replay a captured two-step
 // graph (the ping-pong parity returns to its start after two steps for every
-// integrator), a leftover single step and profiled runs launch directly.
+// integrator), a leftover single step replays a one-step graph of its
+// starting buffer (the streaming call nexd_step_io runs one step at a time);
+// profiled runs launch kernel by kernel.
 int enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
   c->movie_last_it = std::max(c->movie_last_it, it_end);
   set_step_kernel<<<1, 32, 0, c->stream>>>(c->it_dev, it_begin);
   int n = it_end - it_begin + 1;
-  if (c->profiling || !c->use_graphs || n < 2) {
+  if (c->profiling || !c->use_graphs) {
     enqueue_body(c, n);
     return NEXD_OK;
   }
@@ -1026,25 +1084,27 @@ int enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
     c->graph_energy = c->energy_on;
   }
   const int p = c->cur;
-  if (!c->gexec[p]) {
-    const int64_t before = c->launches;
-    cudaGraph_t g = nullptr;
-    CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_body(c, 2);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    c->graph_launches = int(c->launches - before);  // kernels in the captured graph
-    c->launches = before;                           // counted when the graph runs
-    if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&c->gexec[p], g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-    if (c->cur != p) return set_err(c, NEXD_ERR_CUDA, "two-step graph changed the buffer parity");
+  if (n >= 2) {
+    if (!c->gexec[p]) {
+      if (int st = capture_steps(c, 2, &c->gexec[p], &c->graph_launches)) return st;
+      if (c->cur != p) return set_err(c, NEXD_ERR_CUDA, "two-step graph changed the buffer parity");
+    }
+    for (; n >= 2; n -= 2) {
+      CUDA_TRY(c, cudaGraphLaunch(c->gexec[p], c->stream));
+      c->launches += c->graph_launches;
+    }
   }
-  for (; n >= 2; n -= 2) {
-    CUDA_TRY(c, cudaGraphLaunch(c->gexec[p], c->stream));
-    c->launches += c->graph_launches;
+  if (n == 1) {
+    const int q = c->cur;
+    if (!c->gexec1[q]) {
+      if (int st = capture_steps(c, 1, &c->gexec1[q], &c->graph1_launches[q])) return st;
+      c->gend1[q] = c->cur;  // capture advanced the host-side buffer index
+      c->cur = q;
+    }
+    CUDA_TRY(c, cudaGraphLaunch(c->gexec1[q], c->stream));
+    c->launches += c->graph1_launches[q];
+    c->cur = c->gend1[q];
   }
-  if (n == 1) enqueue_body(c, 1);
   return NEXD_OK;
 }
 
@@ -1087,10 +1147,7 @@ int nexd_step_io(nexd_ctx* c, int32_t it, const float* stf_in, float* traces_out
   if (!c || !traces_out) return set_err(c, NEXD_ERR_INVALID, "null argument");
   if (it < 1 || it > c->nt) return set_err(c, NEXD_ERR_INVALID, "step out of 1..nt");
   const size_t nin = size_t(c->nspt) * c->nsrc, nout = size_t(c->nrec) * 9 * c->nbatch;
-  if (!c->pinned) {
-    c->pinned_floats = std::max<size_t>(1, nin + nout);
-    CUDA_TRY(c, cudaMallocHost(&c->pinned, c->pinned_floats * sizeof(float)));
-  }
+  if (!c->pinned || c->pinned_floats < nin + nout) return set_err(c, NEXD_ERR_INVALID, "no pinned staging buffer");
   if (stf_in && nin > 0) {
     std::memcpy(c->pinned, stf_in, nin * sizeof(float));
     // row s of (nspt, nsrc) goes to stf[s][it-1][:]
@@ -1821,6 +1878,15 @@ extern "C" {
 int nexd_wavefield_energy_noalloc(const float* q, int64_t ldq, int32_t nelem, int32_t Np, int32_t nbatch,
                                   const float* emat, const double* mass, int32_t formula, double* energy) {
   if (!q || !emat || !mass || !energy) return set_err(nullptr, NEXD_ERR_INVALID, "null argument");
+  // The kernel reads emat as 16-byte vectors, mass as FP64 and q as FP32: a
+  // misaligned caller pointer (a pool sub-allocation or a tensor view at an
+  // odd offset) would fault the GPU, so it is refused before any launch.
+  if (reinterpret_cast<uintptr_t>(emat) % 16 != 0)
+    return set_err(nullptr, NEXD_ERR_INVALID, "emat must be 16-byte aligned (read as float4)");
+  if (reinterpret_cast<uintptr_t>(mass) % 8 != 0)
+    return set_err(nullptr, NEXD_ERR_INVALID, "mass must be 8-byte aligned (FP64)");
+  if (reinterpret_cast<uintptr_t>(q) % 4 != 0 || reinterpret_cast<uintptr_t>(energy) % 8 != 0)
+    return set_err(nullptr, NEXD_ERR_INVALID, "q must be 4-byte aligned and energy 8-byte aligned");
   if (nelem < 1 || Np < 1 || Np > kEnergyThreads || ldq < int64_t(nelem) * Np)
     return set_err(nullptr, NEXD_ERR_INVALID, "bad sizes (need nelem >= 1, 1 <= Np <= 256, ldq >= nelem*Np)");
   if (nbatch < 1 || nbatch > NEXD_NOALLOC_MAX_BATCH)
@@ -1864,10 +1930,21 @@ int nexd_wavefield_energy_noalloc(const float* q, int64_t ldq, int32_t nelem, in
   ea.mass = mass;
   ea.partials = partials;
   ea.formula = formula;
-  energy_kernel<<<dim3(nblk, nbatch), kEnergyThreads, smem, 0>>>(ea);
-  noalloc_sum<<<nbatch, 256, 0, 0>>>(partials, nblk, totals);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return set_err(nullptr, NEXD_ERR_CUDA, std::string("energy launch: ") + cudaGetErrorString(e));
+  // Launched through cudaLaunchKernel so that each launch's own status is
+  // checked: an earlier error left in the runtime by the host's other CUDA
+  // code is neither reported as this call's failure nor cleared.
+  int nparts = nblk;
+  void* energy_params[] = {&ea};
+  void* sum_params[] = {&partials, &nparts, &totals};
+  cudaError_t e = cudaLaunchKernel(reinterpret_cast<const void*>(&energy_kernel), dim3(nblk, nbatch),
+                                   dim3(kEnergyThreads), energy_params, smem, nullptr);
+  if (e == cudaSuccess)
+    e = cudaLaunchKernel(reinterpret_cast<const void*>(&noalloc_sum), dim3(nbatch), dim3(256), sum_params, 0,
+                         nullptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // the launch error is this call's own
+    return set_err(nullptr, NEXD_ERR_CUDA, std::string("energy launch: ") + cudaGetErrorString(e));
+  }
   e = cudaMemcpy(energy, totals, size_t(nbatch) * sizeof(double), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return set_err(nullptr, NEXD_ERR_CUDA, std::string("energy copy: ") + cudaGetErrorString(e));
   return NEXD_OK;

@@ -55,12 +55,19 @@ struct Order {
   static constexpr int SL = 4 * NPAIR * Np * 2; // LIFT as [face][pair][n][2]
   // one prefetch buffer: element records, own wavefield (field-major), the
   // neighbour face traces and the connectivity of the following chunk
-  // element records at a 68-word stride: the same field of different
-  // elements in one warp falls on different banks (a 64-word stride puts it
-  // on one bank)
-  static constexpr int GSTR = 68;
+  // element records (80 words) at an 84-word stride: the same field of
+  // the elements that share a warp falls on different banks (84 = 20 mod 32;
+  // an 80-word stride would put elements 0 and 2 on one bank)
+  static constexpr int GSTR = 84;
   static constexpr int SGEO = E * GSTR;
-  static constexpr int SQF = r4(9 * E * Np);
+  // Own wavefield: one slot of QF floats per field holding the chunk's node
+  // range [e0 Np, (e0 + ne) Np) widened to 16-byte boundaries (at most E Np
+  // + 6 floats; none when Np is a multiple of 4), copied as QCH 16-byte
+  // pieces per field; the chunk's first node sits at offset (e0 Np) mod 4.
+  static constexpr int pow2ceil(int x) { return x <= 1 ? 1 : 2 * pow2ceil((x + 1) / 2); }
+  static constexpr int QCH = pow2ceil((E * Np + (Np % 4 ? 6 : 0) + 3) / 4);
+  static constexpr int QF = 4 * QCH;
+  static constexpr int SQF = 9 * QF;
   static constexpr int STR = r4(E * NF * 9);
   static constexpr int SIDS = r4(E * 12);
   static constexpr int BUF = SGEO + SQF + STR + SIDS;
@@ -105,7 +112,10 @@ enum GeoOffset {
   G_IZS = 61,  // 1/(rho vs)
   G_AP = 62,   // 1/(lambda+2mu)
   G_AS = 63,   // 1/(2mu)
-  GEO_STRIDE = 64
+  G_AEL = 64,  // Zener coefficients of mechanism l: -lam Ylam, -2mu Ymu, their sum (64 + 3l ..)
+  G_SRC = 73,  // first source of the element (int bits), -1 for none
+  G_SLOT = 74, // receiver slot of the element (int bits), -1 for none
+  GEO_STRIDE = 80
 };
 
 enum StageMode { MODE_LSERK = 0, MODE_TVD = 1 };
@@ -126,6 +136,7 @@ struct StageArgs {
   int npat;
   const float* ael;    // [K][3*nMB]: -lam*Ylam, -2mu*Ymu, sum (src/timeloopMod.f90:274-282)
   const float* wl;     // [nMB]
+  float wlv[3];        // the relaxation frequencies as kernel parameters
   const float* prof;   // [Kpml][9][Np]: ddx ddy ddz ax ay az kx ky kz
   // state, batch member b at offset b*9*ldq (q/res), b*6*nMB*ldt (theta), b*27*lda (aux)
   const float* q_in;
@@ -291,13 +302,17 @@ __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, f
   constexpr int Np = O::Np, E = O::E;
   const int tid = threadIdx.x, nth = blockDim.x;
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
-  for (int i = tid; i < c.ne * 16; i += nth)
-    cp_async16(bGeo + (i >> 4) * O::GSTR + 4 * (i & 15), a.geo + (long long)c.e0 * GEO_STRIDE + 4 * i);
-  const int cnt = c.ne * Np;
+  for (int i = tid; i < c.ne * (GEO_STRIDE / 4); i += nth)
+    cp_async16(bGeo + (i / (GEO_STRIDE / 4)) * O::GSTR + 4 * (i % (GEO_STRIDE / 4)),
+               a.geo + (long long)c.e0 * GEO_STRIDE + 4 * i);
+  // per field the 16-byte pieces of [base, base + cnt) widened to 16-byte
+  // boundaries; in bounds: the field stride ldq is a multiple of 64 nodes
   const long long base = (long long)c.e0 * Np;
-  for (int i = tid; i < 9 * E * Np; i += nth) {
-    const int f = i / (E * Np), r = i - f * (E * Np);
-    if (r < cnt) cp_async4(bQ + i, qin + f * a.ldq + base + r);
+  const long long s0 = base & ~3LL;
+  const int npiece = int((base + c.ne * Np + 3 - s0) >> 2);
+  for (int i = tid; i < 9 * O::QCH; i += nth) {
+    const int f = i / O::QCH, j = i - f * O::QCH;
+    if (j < npiece) cp_async16(bQ + f * O::QF + 4 * j, qin + f * a.ldq + s0 + 4 * j);
   }
   if (next)
     for (int i = tid; i < next->ne * 2; i += nth) {
@@ -362,11 +377,11 @@ struct NodePrefetch {
   float ae[(ATT && EARLY) ? 3 * kNMB : 1];  // per-element Zener coefficients
   int src, slot, pml_off;                   // first source of the element, receiver slot, NPML switched off
 
-  __device__ __forceinline__ const float* zener(const StageArgs& a, int e) const {
-    return EARLY ? ae : a.ael + (long long)e * 3 * kNMB;
-  }
-  __device__ __forceinline__ int first_source(const StageArgs& a, int e) const { return EARLY ? src : a.src_head[e]; }
-  __device__ __forceinline__ int receiver_slot(const StageArgs& a, int e) const { return EARLY ? slot : a.rec_slot[e]; }
+  // g: the element's record in shared memory (Zener coefficients, first
+  // source and receiver slot are part of it)
+  __device__ __forceinline__ const float* zener(const float* g) const { return EARLY ? ae : g + G_AEL; }
+  __device__ __forceinline__ int first_source(const float* g) const { return EARLY ? src : __float_as_int(g[G_SRC]); }
+  __device__ __forceinline__ int receiver_slot(const float* g) const { return EARLY ? slot : __float_as_int(g[G_SLOT]); }
   __device__ __forceinline__ bool npml_off(const StageArgs& a, int b) const { return EARLY ? pml_off != 0 : a.pml_off[b] != 0; }
 
   template <int Np>
@@ -490,15 +505,15 @@ __device__ __forceinline__ void elastic_fluxes(const float* g, const float* qv, 
 template <int Np, bool ATT, bool PML, int MODE, bool EARLY>
 __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, long long node, float* rq, const float* S,
                                             const NodePrefetch<ATT, PML, MODE, EARLY>& p, const float* qown,
-                                            int qstride, const float* wls) {
+                                            int qstride, const float* g) {
   const int n = int(node - (long long)e * Np);
   if (ATT) {
     float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
     float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
-    const float* ae = p.zener(a, e);
+    const float* ae = p.zener(g);
 #pragma unroll
     for (int l = 0; l < kNMB; ++l) {
-      const float wl = EARLY ? wls[l] : a.wl[l];
+      const float wl = a.wlv[l];
       const float* t = p.th + 6 * l;
       const float* t2 = p.th2 + 6 * l;
       const float c1 = ae[3 * l], c2 = ae[3 * l + 1], c3 = ae[3 * l + 2];
@@ -526,7 +541,7 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
       }
     }
   }
-  for (int s = p.first_source(a, e); s >= 0; s = a.src_next[s]) {
+  for (int s = p.first_source(g); s >= 0; s = a.src_next[s]) {
     if (a.src_batch[s] != b) continue;
     const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
     const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
@@ -535,7 +550,7 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
     for (int c = 0; c < 9; ++c) rq[c] = fmaf(sp[c * Np], amp, rq[c]);
   }
   if (a.last_stage) {
-    const int slot = p.receiver_slot(a, e);
+    const int slot = p.receiver_slot(g);
     if (slot >= 0) {
       float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
       ab[0] = rq[6];
@@ -582,7 +597,6 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       sAmp[(i >> 2) / 3 * O::AE + (i >> 2) % 3 * O::NFP + (i & 3) * 2 * O::NPAIR + NpF] = 0.f;
   for (int i = tid; i < a.npat * NpF; i += blockDim.x) sPat[i] = a.patterns[i];
 
-  const float* wls = nullptr;  // relaxation frequencies are read from a.wl where used
   const int nel = a.e_end - a.e_begin;
   const int nchunk = (nel + E - 1) / E;
   const int nwork = nchunk * a.nbatch;
@@ -624,8 +638,9 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     const int b = ch.b, e0 = ch.e0, ne = ch.ne;
     float* buf = sBuf + p * O::BUF;
     const float* sGeo = buf;
-    const float* sQF = buf + O::SGEO;
-    const float* sTr = sQF + O::SQF;
+    const float* sTr = buf + O::SGEO + O::SQF;
+    // own wavefield of the chunk: field c of node n of element le at sQF[c * QF + le * Np + n]
+    const float* sQF = buf + O::SGEO + int(((long long)e0 * Np) & 3);
     const int* sIds = reinterpret_cast<const int*>(sTr + O::STR);  // connectivity of the next chunk
     cp_async_wait_all();
     __syncthreads();  // this chunk's data is in `buf`; the other buffer and work areas are free
@@ -654,7 +669,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       // at a 12-word stride touches 32 different banks
       float* dst = sQI + le * O::QE + n * QS;
       const float* src = sQF + le * Np + n;
-      constexpr int FS = E * Np;
+      constexpr int FS = O::QF;
       *reinterpret_cast<float4*>(dst) = make_float4(src[0], src[FS], src[2 * FS], src[3 * FS]);
       *reinterpret_cast<float4*>(dst + 4) = make_float4(src[4 * FS], src[5 * FS], src[6 * FS], src[7 * FS]);
       dst[8] = src[8 * FS];
@@ -668,7 +683,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       const int own = sPat[f * NpF + fi];  // patterns 0..3 are the element's own face masks
       const float* qo = sQF + ee * Np + own;
       float dq[9];
-      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, E * Np, dq);
+      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, O::QF, dq);
       float ap, as1, as2;
       face_amplitudes(g, f, dq, free_face, ap, as1, as2);
       const float fs = g[G_FS + f];
@@ -685,7 +700,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       const float* g = sGeo + le * O::GSTR;
       float qv[9];
 #pragma unroll
-      for (int c = 0; c < 9; ++c) qv[c] = sQF[c * (E * Np) + le * Np + n];
+      for (int c = 0; c < 9; ++c) qv[c] = sQF[c * O::QF + le * Np + n];
       float F[9], G[9], H[9];
       elastic_fluxes(g, qv, F, G, H);
       pml_node<ATT, MODE>(a, b, node, pf, F, G, H);
@@ -796,8 +811,8 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
         const float* c8 = cfe + k * CS + 8;
         acc8 = fmaf(d.x, c8[0], fmaf(d.y, c8[10], fmaf(d.z, c8[20], acc8)));
         if (ATT) {
-          const float2 v01 = make_float2(qv[6 * (E * Np) + k], qv[7 * (E * Np) + k]);
-          const float v2 = qv[8 * (E * Np) + k];
+          const float2 v01 = make_float2(qv[6 * O::QF + k], qv[7 * O::QF + k]);
+          const float v2 = qv[8 * O::QF + k];
           v01r = __ffma2_rn(d0, v01, v01r);
           v01s = __ffma2_rn(d1, v01, v01s);
           v01t = __ffma2_rn(d2, v01, v01t);
@@ -858,7 +873,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       S[4] = sig_an[4] - 0.5f * (vgrad[7] + vgrad[5]);
       S[5] = sig_an[5] - 0.5f * (vgrad[6] + vgrad[2]);
     }
-    finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, E * Np, wls);
+    finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, O::QF, g);
   }
   cp_async_wait_all();
 }

@@ -103,8 +103,9 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
     const int b = ch.b, e0 = ch.e0, ne = ch.ne;
     float* buf = sBuf + p * O::BUF;
     const float* sGeo = buf;
-    const float* sQF = buf + O::SGEO;
-    const float* sTr = sQF + O::SQF;
+    const float* sTr = buf + O::SGEO + O::SQF;
+    // own wavefield of the chunk: field c of node n of element le at sQF[c * QF + le * Np + n]
+    const float* sQF = buf + O::SGEO + int(((long long)e0 * Np) & 3);
     const int* sIds = reinterpret_cast<const int*>(sTr + O::STR);
     cp_async_wait_all();
     __syncthreads();
@@ -130,10 +131,10 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
     if (active) {
       float* dst = sQI + le * O::QE;
 #pragma unroll
-      for (int c = 0; c < 9; ++c) dst[n1 * QS + c] = sQF[c * (E * Np) + le * Np + n1];
+      for (int c = 0; c < 9; ++c) dst[n1 * QS + c] = sQF[c * O::QF + le * Np + n1];
       if (has2) {
 #pragma unroll
-        for (int c = 0; c < 9; ++c) dst[n2 * QS + c] = sQF[c * (E * Np) + le * Np + n2];
+        for (int c = 0; c < 9; ++c) dst[n2 * QS + c] = sQF[c * O::QF + le * Np + n2];
       }
     }
     for (int i = tid; i < ne * NF; i += blockDim.x) {
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
       const int own = sPat[f * NpF + fi];
       const float* qo = sQF + ee * Np + own;
       float dq[9];
-      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, E * Np, dq);
+      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, O::QF, dq);
       float ap, as1, as2;
       face_amplitudes(g, f, dq, free_face, ap, as1, as2);
       const float fs = g[G_FS + f];
@@ -230,10 +231,10 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
     };
     float S[6];
     if (ATT) strain(sa1, vg1, S);
-    finish_node<Np, ATT, false, MODE>(a, b, e, base + n1, rq1, S, pf1, sQF + le * Np + n1, E * Np, nullptr);
+    finish_node<Np, ATT, false, MODE>(a, b, e, base + n1, rq1, S, pf1, sQF + le * Np + n1, O::QF, g);
     if (has2) {
       if (ATT) strain(sa2, vg2, S);
-      finish_node<Np, ATT, false, MODE>(a, b, e, base + n2, rq2, S, pf2, sQF + le * Np + n2, E * Np, nullptr);
+      finish_node<Np, ATT, false, MODE>(a, b, e, base + n2, rq2, S, pf2, sQF + le * Np + n2, O::QF, g);
     }
   }
   cp_async_wait_all();

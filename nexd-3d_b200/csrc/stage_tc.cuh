@@ -83,9 +83,6 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
   const int nwork = nchunk * a.nbatch;
   int w = blockIdx.x;
   if (w >= nwork) return;
-  float wls[kNMB];
-#pragma unroll
-  for (int l = 0; l < kNMB; ++l) wls[l] = ATT ? __ldg(a.wl + l) : 0.f;
 
   for (int i = tid; i < int(T::B_BYTES / 16); i += blockDim.x) reinterpret_cast<uint4*>(sB)[i] = ops[i];
   for (int i = tid; i < int(3 * T::A_BYTES / 16); i += blockDim.x) reinterpret_cast<uint4*>(sA)[i] = make_uint4(0, 0, 0, 0);
@@ -139,14 +136,15 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
     const Chunk ch = chunk_of<E>(a, w, nchunk);
     const int b = ch.b, e0 = ch.e0, ne = ch.ne;
     const float* sGeo = geo_of(p);
-    const float* sQF = q_of(p);
+    // own wavefield of the chunk: field c of node n of element le at sQF[c * QF + le * Np + n]
+    const float* sQF = q_of(p) + int(((long long)e0 * Np) & 3);
     const int* sIds = ids_of(p);
     cp_async_wait_all();
     __syncthreads();  // chunk data landed; the previous chunk's result buffer is consumed
 
     const bool active = le < ne;
     const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
-    NodePrefetch<ATT, PML, MODE, true> pf;
+    NodePrefetch<ATT, PML, MODE> pf;
     if (active) pf.template load<Np>(a, b, e0 + le, node);
     const int wn = w + gridDim.x;
     Chunk cn;
@@ -164,7 +162,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
       const float* g = sGeo + le * O::GSTR;
       float qv[9];
 #pragma unroll
-      for (int c = 0; c < 9; ++c) qv[c] = sQF[c * (E * Np) + le * Np + n];
+      for (int c = 0; c < 9; ++c) qv[c] = sQF[c * O::QF + le * Np + n];
       float F[9], G[9], H[9];
       elastic_fluxes(g, qv, F, G, H);
       if constexpr (PML) pml_node<ATT, MODE>(a, b, node, pf, F, G, H);
@@ -208,7 +206,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
       const int own = sPat[f * NpF + fi];
       const float* qo = sQF + ee * Np + own;
       float dq[9];
-      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, E * Np, dq);
+      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, O::QF, dq);
       float ap, as1, as2;
       face_amplitudes(g, f, dq, free_face, ap, as1, as2);
       const float fs = g[G_FS + f];
@@ -237,6 +235,10 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
     const bool done = tc::mbar_wait(tc::smem_u32(mbar), phase);
     if (__syncthreads_or(!done)) {
       if (tid == 0) atomicOr(a.flag, 2);
+      // The committed MMAs may still be writing the accumulator: wait once
+      // more, again bounded, for their arrival before the TMEM is released
+      // at the end of the kernel.
+      tc::mbar_wait(tc::smem_u32(mbar), phase, 1u << 24);
       break;
     }
     tc::fence_after_sync();
@@ -284,7 +286,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
 #pragma unroll
         for (int c = 0; c < 6; ++c) S[c] = r[(9 + c) * T::RS];
       }
-      finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, E * Np, wls);
+      finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, O::QF, sGeo + le * O::GSTR);
     }
   }
   cp_async_wait_all();

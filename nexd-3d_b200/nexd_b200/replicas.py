@@ -4,7 +4,10 @@ The time loop shards as independent units (sources, models): every rank
 runs its own replica with its own seeded source, no collective touches the
 data path, and the only collectives are the barrier around the timed region
 and the reductions of the timing (maximum over ranks) and of the work (sum
-over ranks).  The process group uses NCCL on GPUs and gloo on CPUs (tests).
+over ranks).  At the end of a run the receiver traces of every replica are
+gathered on rank 0 (the reference writes each station's seismograms from the
+rank that holds it, src/timeloopMod.f90:591-656; here every rank holds a whole
+replica).  The process group uses NCCL on GPUs and gloo on CPUs (tests).
 """
 import os
 from datetime import timedelta
@@ -57,6 +60,24 @@ def init(backend=None, timeout_s=600):
         return Group(rank, ws, local, dist, device="cuda")
     dist.init_process_group("gloo", timeout=timedelta(seconds=timeout_s))
     return Group(rank, ws, local, dist, device="cpu")
+
+
+def gather_traces(group, traces):
+    """Receiver traces of every rank's replica, stacked in rank order on rank
+    0: array (world, *traces.shape) there, None on the other ranks.  Every
+    rank passes an array of the same shape and dtype (one collective, after
+    the time loop; nothing on the data path)."""
+    import numpy as np
+    arr = np.ascontiguousarray(traces)
+    if group.dist is None:
+        return arr[None].copy()
+    import torch
+    t = torch.from_numpy(arr).to(group.device)
+    parts = [torch.empty_like(t) for _ in range(group.world)] if group.rank == 0 else None
+    group.dist.gather(t, gather_list=parts, dst=0)
+    if group.rank != 0:
+        return None
+    return np.stack([p.cpu().numpy() for p in parts])
 
 
 def replica_seed(base, rank):

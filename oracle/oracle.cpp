@@ -22,6 +22,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -34,6 +35,8 @@
 namespace {
 
 thread_local std::string g_err;
+// seconds spent in the time-step loop of the last oracle_run (set-up excluded)
+thread_local double g_loop_seconds = 0.0;
 
 // Carpenter & Kennedy (1994) five-stage fourth-order 2N-storage coefficients.
 const double kRK4A[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
@@ -609,6 +612,11 @@ struct Oracle {
           for (int j = 0; j < Np; ++j) pmlnode[size_t(e) * Np + j] = 1;
     }
     const size_t toff = size_t(batch) * nrec * nt * 9;
+    const auto loop_start = std::chrono::steady_clock::now();
+    struct LoopTimer {  // adds the time-loop seconds of this run to g_loop_seconds
+      std::chrono::steady_clock::time_point t0;
+      ~LoopTimer() { g_loop_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+    } loop_timer{loop_start};
     for (int it = 1; it <= it_end; ++it) {
       // receivers (src/timeloopMod.f90:358-373)
       for (int r = 0; r < nrec; ++r) {
@@ -682,6 +690,7 @@ struct TriggerCfg {
 
 template <class R>
 int run_t(const nexd_desc* d, int it_end, float* traces, double* field, const TriggerCfg* tc = nullptr) {
+  g_loop_seconds = 0.0;
   Oracle<R> o(*d);
   std::fill(traces, traces + size_t(d->nrec) * d->nt * 9 * std::max(1, d->nbatch), 0.0f);
   const int nb = std::max(1, d->nbatch);
@@ -775,6 +784,8 @@ int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const doubl
     return NEXD_ERR_INVALID;
   }
 }
+
+double oracle_loop_seconds() { return g_loop_seconds; }
 
 int oracle_last_error(char* buf, size_t len) {
   if (!buf || !len) return NEXD_ERR_INVALID;

@@ -45,6 +45,11 @@ int oracle_run_trigger(const nexd_desc* d, int precision, int it_end, float* tra
 
 int oracle_last_error(char* buf, size_t len);
 
+/* Seconds the last oracle_run / oracle_run_trigger on this thread spent in its
+ * time-step loop (operator and state set-up excluded): the CPU baseline's
+ * timed region. */
+double oracle_loop_seconds(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,4 +58,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python make_brick_fixture.py <path of the NEXD-3D source tree>")
+    main(sys.argv[1])

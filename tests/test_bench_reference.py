@@ -33,7 +33,9 @@ def test_reference_arm_under_two_ranks():
     d = lines[0]
     assert d["impl"] == "reference" and d["metric"] == "DOF-stage updates/s" and d["unit"] == "DOF-stage/s"
     assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 2
+    # the same workload as the GPU arm: the full 192,000-tet model, not a smaller sample
+    assert d["config"]["workload"] == "twolayer_anelastic_npml_192k_tets_N4_lserk4" and d["config"]["tets"] == 192000
     cb = d["cpu_baseline"]
-    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and "192000 tets" in cb["sample"]
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0

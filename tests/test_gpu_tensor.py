@@ -179,7 +179,7 @@ def test_autotune_leaves_state_and_picks_valid_kinds(tmp_path, oracle, Solver, t
     assert trace_misfit(s.traces()[..., 0], run_oracle(oracle, m, 64)[..., 0]) < 1e-4
 
 
-@pytest.mark.parametrize("N", [3, 4])
+@pytest.mark.parametrize("N", [2, 3, 4, 5])
 def test_node_pair_kernel_is_bit_identical(tmp_path, Solver, N):
     """The node-pair FP32 kernel (elements outside the NPML) performs the
     FP32 kernel's operations in the same order: identical wavefields, memory

@@ -1,11 +1,12 @@
 """The CPU oracle (oracle/liboracle.so) pinned against the reference's own
 golden seismograms and checked for the properties the method guarantees."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
 
-from conftest import (brick_dt_cfl, pin_brick_edge_stations, run_oracle, run_oracle_trigger, trace_misfit,
+from conftest import (GOLDEN, brick_dt_cfl, pin_brick_edge_stations, run_oracle, run_oracle_trigger, trace_misfit,
                       station_misfit, write_brick, rel_l2)
 from nexd_b200 import Mesh, synth
 
@@ -128,3 +129,18 @@ def test_pml_energy_and_trigger(tmp_path, oracle):
     # averages overflow, the ratio is NaN and the trigger never fires.
     tr3, en3, sw3 = run_oracle_trigger(oracle, m, 64, thr=1e-9, f0=f0, formula=0)
     assert sw3[0] == 0 and np.isfinite(en3).all()
+
+
+@pytest.mark.parametrize("name", ["cube", "twolayer"])
+def test_fullrun_fixture_matches_oracle_prefix(tmp_path, oracle, name):
+    """The full-run FP64 trace fixtures (tests/golden/fullrun_*.npz) belong to
+    the meshes the generator rebuilds: same descriptor fingerprint, and the
+    oracle's first 60 steps reproduce the stored traces' first 60 steps."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_fullrun_fixtures as fx
+    ref = np.load(os.path.join(GOLDEN, f"fullrun_{name}.npz"))
+    m = fx.build(name, str(tmp_path / name))
+    assert np.allclose(fx.fingerprint(m), ref["fingerprint"], rtol=1e-12, atol=0)
+    tr = run_oracle(oracle, m, 64, steps=60)[..., 0]
+    assert np.array_equal(tr[:, :60], ref["traces"][:, :60])

@@ -34,8 +34,16 @@ def _rank_main(rank, world, port, out_dir):
     d = os.path.join(out_dir, f"r{rank}")
     synth.write_twolayer(d, cells=(6, 6, 3), nt=5, nrec=2, src_seed=replicas.replica_seed(2, rank))
     src = open(os.path.join(d, "data", "source")).read()
+    # end of run: each replica's receiver traces (nrec, nt, 9, nbatch) gathered on rank 0
+    traces = np.full((2, 5, 9, 1), float(rank + 1), dtype=np.float32, order="F")
+    traces[0, :, 0, 0] = np.arange(5) + 10 * rank
+    gathered = replicas.gather_traces(g, traces)
     g.barrier()
     g.close()
+    if rank == 0:
+        np.save(os.path.join(out_dir, "gathered.npy"), gathered)
+    else:
+        assert gathered is None
     np.save(os.path.join(out_dir, f"res{rank}.npy"), np.array([res["max"], res["sum"], res["agg"]]))
     with open(os.path.join(out_dir, f"src{rank}.txt"), "w") as f:
         f.write(src)
@@ -50,6 +58,12 @@ def test_two_gloo_ranks(tmp_path):
     assert r0[0] == 2.0 and r0[1] == 300.0 and np.isclose(r0[2], 150.0)
     # each rank's replica has its own seeded source
     assert open(tmp_path / "src0.txt").read() != open(tmp_path / "src1.txt").read()
+    # rank 0 holds every replica's traces in rank order
+    gathered = np.load(tmp_path / "gathered.npy")
+    assert gathered.shape == (2, 2, 5, 9, 1)
+    for r in range(world):
+        assert np.all(gathered[r, 1] == r + 1)
+        assert np.array_equal(gathered[r, 0, :, 0, 0], np.arange(5) + 10 * r)
 
 
 def test_single_process_group_is_local():
@@ -59,6 +73,7 @@ def test_single_process_group_is_local():
     try:
         g = replicas.init()
         assert g.dist is None and g.world == 1
+        assert replicas.gather_traces(g, np.ones((2, 3))).shape == (1, 2, 3)
         assert g.max(3.0) == 3.0 and g.sum(5.0) == 5.0 and replicas.aggregate(g, 10.0, 2.0) == 5.0
         g.barrier()
         g.close()
