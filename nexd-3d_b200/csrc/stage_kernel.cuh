@@ -277,6 +277,13 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+// 16 bytes through L1 (.ca): tetrahedra of one hexahedron sit next to each
+// other in the element order, so many neighbour face traces of a chunk are
+// nodes of the same chunk and hit the lines its own-wavefield copies brought in
+__device__ __forceinline__ void cp_async16_ca(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -312,7 +319,7 @@ __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, f
   const int npiece = int((base + c.ne * Np + 3 - s0) >> 2);
   for (int i = tid; i < 9 * O::QCH; i += nth) {
     const int f = i / O::QCH, j = i - f * O::QCH;
-    if (j < npiece) cp_async16(bQ + f * O::QF + 4 * j, qin + f * a.ldq + s0 + 4 * j);
+    if (j < npiece) cp_async16_ca(bQ + f * O::QF + 4 * j, qin + f * a.ldq + s0 + 4 * j);
   }
   if (next)
     for (int i = tid; i < next->ne * 2; i += nth) {

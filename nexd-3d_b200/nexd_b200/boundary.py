@@ -120,28 +120,42 @@ def init_params(nin, hidden=HIDDEN, seed=0):
 # wide / small model pair
 # ---------------------------------------------------------------------------
 
+def _default_layers(Lz):
+    return [(Lz - 600.0, 3000.0, 1730.0, 2400.0, 9000.0, 9000.0), (-np.inf, 5000.0, 2890.0, 2800.0, 9000.0, 9000.0)]
+
+
+def write_npml_model(directory, *, cells, h, pml_cells, nt, sources=(), stations=(), layers=None):
+    """The small model's box surrounded by pml_cells of NPML on the sides and
+    the bottom (free top), with the same undistorted tetrahedra inside.
+    Returns the element index (0-based) of every small-model element in it."""
+    nx, ny, nz = cells
+    P = pml_cells
+    Lx, Ly, Lz = nx * h, ny * h, nz * h
+    layers = layers or _default_layers(Lz)
+    par = dict(timeint=4, nt=nt, cfl=0.3, set_pml=".true.", pml_delta=P * h, pml_rc=0.001, pml_kmax=1.0,
+               pml_afac=1.0)
+    W = (nx + 2 * P, ny + 2 * P, nz + P)
+    synth.write_simulation(directory, box=(-P * h, Lx + P * h, -P * h, Ly + P * h, -P * h, Lz), cells=W, jitter=0.0,
+                           layers=layers, pml_cells=P, parfile=par, sources=sources, stations=stations)
+    hex_small = np.arange(nx * ny * nz)
+    i, j, k = hex_small % nx, (hex_small // nx) % ny, hex_small // (nx * ny)
+    hex_wide = (i + P) + W[0] * ((j + P) + W[1] * (k + P))
+    return (hex_wide[:, None] * 6 + np.arange(6)[None, :]).ravel()
+
+
 def write_model_pair(wide_dir, small_dir, *, cells=(8, 8, 4), h=250.0, pml_cells=8, nt=300, sources=(),
                      stations=(), layers=None, f0=3.0):
     """Small model (cells, absorbing sides and bottom, free top) and the wide
     model around it (pml_cells of NPML on the sides and the bottom), with the
     same undistorted tetrahedra inside.  Returns wide element index (0-based)
     of every small element."""
-    nx, ny, nz = cells
-    P = pml_cells
-    Lx, Ly, Lz = nx * h, ny * h, nz * h
-    layers = layers or [(Lz - 600.0, 3000.0, 1730.0, 2400.0, 9000.0, 9000.0),
-                        (-np.inf, 5000.0, 2890.0, 2800.0, 9000.0, 9000.0)]
+    Lz = cells[2] * h
+    layers = layers or _default_layers(Lz)
     par = dict(timeint=4, nt=nt, cfl=0.3)
-    synth.write_simulation(small_dir, box=(0.0, Lx, 0.0, Ly, 0.0, Lz), cells=cells, jitter=0.0, layers=layers,
-                           parfile=par, sources=sources, stations=stations)
-    wpar = dict(par, set_pml=".true.", pml_delta=P * h, pml_rc=0.001, pml_kmax=1.0, pml_afac=1.0)
-    W = (nx + 2 * P, ny + 2 * P, nz + P)
-    synth.write_simulation(wide_dir, box=(-P * h, Lx + P * h, -P * h, Ly + P * h, -P * h, Lz), cells=W, jitter=0.0,
-                           layers=layers, pml_cells=P, parfile=wpar, sources=sources, stations=stations)
-    hex_small = np.arange(nx * ny * nz)
-    i, j, k = hex_small % nx, (hex_small // nx) % ny, hex_small // (nx * ny)
-    hex_wide = (i + P) + W[0] * ((j + P) + W[1] * (k + P))
-    return (hex_wide[:, None] * 6 + np.arange(6)[None, :]).ravel()
+    synth.write_simulation(small_dir, box=(0.0, cells[0] * h, 0.0, cells[1] * h, 0.0, Lz), cells=cells, jitter=0.0,
+                           layers=layers, parfile=par, sources=sources, stations=stations)
+    return write_npml_model(wide_dir, cells=cells, h=h, pml_cells=pml_cells, nt=nt, sources=sources,
+                            stations=stations, layers=layers)
 
 
 def record_pairs(wide_solver, wide_elem, face, steps, npf, every=1):
@@ -281,9 +295,11 @@ def surface_stations(cells, h, n=9):
 
 
 class ModelPair:
-    """A small (absorbing) model and its wide-NPML extension for one source."""
+    """A small (absorbing) model and its wide-NPML extension for one source;
+    with npml_cells, also the small model inside a thin NPML of that many
+    elements (the layer the learned boundary is meant to replace)."""
 
-    def __init__(self, root, name, source, *, cells, h, pml_cells, duration, N=4, layers=None):
+    def __init__(self, root, name, source, *, cells, h, pml_cells, duration, N=4, layers=None, npml_cells=0):
         from .host import Mesh
         self.wide_dir = os.path.join(root, f"{name}_wide")
         self.small_dir = os.path.join(root, f"{name}_small")
@@ -299,6 +315,15 @@ class ModelPair:
         self.small = Mesh(self.small_dir, N=N, stf_stage_time=True)
         self.wide = Mesh(self.wide_dir, N=N, stf_stage_time=True)
         self.nt = nt
+        self.npml = None
+        if npml_cells:
+            self.npml_dir = os.path.join(root, f"{name}_npml{npml_cells}")
+            self.npml_map = write_npml_model(self.npml_dir, cells=cells, h=h, pml_cells=npml_cells, nt=nt,
+                                             sources=[source], stations=st, layers=layers)
+            self.npml = Mesh(self.npml_dir, N=N, stf_stage_time=True)
+        # kinetic-energy weights of the small model: 1/2 rho J M (M the reference mass matrix)
+        self._mass = np.linalg.inv(self.small.array("invmass"))
+        self._rhoj = 0.5 * self.small.array("rho") * np.abs(self.small.array("jacobian"))
         face = self.small.array("face")
         e, f = np.nonzero(face.T == -2)
         self.bf_small_elem, self.bf_face = e + 1, f + 1
@@ -319,18 +344,36 @@ class ModelPair:
         keep = r > quiet * r.max()
         return xn[keep].astype(np.float32), yn[keep].astype(np.float32)
 
-    def field_on_small(self, wide_field):
+    def field_on_small(self, wide_field, emap=None):
         Np = self.small.Np
-        idx = (self.map[:, None] * Np + np.arange(Np)[None, :]).ravel()
+        emap = self.map if emap is None else emap
+        idx = (emap[:, None] * Np + np.arange(Np)[None, :]).ravel()
         return wide_field[idx]
 
+    def kinetic_energy(self, v):
+        """Kinetic energy of a velocity field on the small model's nodes,
+        v (K Np, 3): sum over elements of 1/2 rho J v_c^T M v_c."""
+        Np = self.small.Np
+        ve = v.reshape(-1, Np, 3)
+        return float(np.einsum("e,enc,nm,emc->", self._rhoj, ve, self._mass, ve))
+
     def evaluate(self, Solver, params, checkpoints, max_reflection=0.5):
-        """Relative L2 of the small model's velocity field against the wide model
-        (restricted to the small domain) at the checkpoint steps, and the trace
-        misfit at the surface stations, for the plain and the learned boundary."""
+        """Every boundary against the wide NPML run (the reference solution) in
+        the small domain: the plain absorbing faces, the learned boundary and,
+        when the pair has one, the thin NPML.  Per boundary: the relative L2 of
+        the velocity field at the checkpoint steps, the trace misfit of the
+        surface stations, and the reflection energy -- the kinetic energy of
+        the difference from the reference inside the small domain (inside it
+        every model solves the same equations, so the difference is what its
+        boundary sent back), as a fraction of the largest kinetic energy of the
+        reference in the small domain at the checkpoints."""
         runs = {}
-        for label, p in (("wide", None), ("plain", None), ("learned", params)):
-            mesh = self.wide if label == "wide" else self.small
+        cases = [("wide", None), ("plain", None), ("learned", params)]
+        if self.npml is not None:
+            cases.append(("npml", None))
+        for label, p in cases:
+            mesh = {"wide": self.wide, "npml": self.npml}.get(label, self.small)
+            emap = {"wide": self.map, "npml": getattr(self, "npml_map", None)}.get(label)
             s = Solver(mesh.desc_ptr)
             if label == "learned":
                 s.set_boundary_mlp(p, max_reflection)
@@ -339,17 +382,19 @@ class ModelPair:
                 s.run(it0, cp)
                 it0 = cp + 1
                 f = s.field()[:, 6:9].astype(np.float64)
-                fields.append(self.field_on_small(f) if label == "wide" else f)
+                fields.append(self.field_on_small(f, emap) if emap is not None else f)
             if it0 <= self.nt:
                 s.run(it0, self.nt)
             runs[label] = (fields, s.traces()[..., 0].astype(np.float64))
             s.close()
         out = {}
         wf, wt = runs["wide"]
-        for label in ("plain", "learned"):
+        e_ref = max(self.kinetic_energy(b) for b in wf)
+        for label, _ in cases[1:]:
             f, t = runs[label]
             out[label] = {
                 "field_err": [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(f, wf)],
                 "trace_err": float(np.linalg.norm(t[:, :, 3:6] - wt[:, :, 3:6]) / np.linalg.norm(wt[:, :, 3:6])),
+                "reflection_energy": [self.kinetic_energy(a - b) / e_ref for a, b in zip(f, wf)],
             }
         return out

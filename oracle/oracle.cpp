@@ -37,6 +37,10 @@ namespace {
 thread_local std::string g_err;
 // seconds spent in the time-step loop of the last oracle_run (set-up excluded)
 thread_local double g_loop_seconds = 0.0;
+// Reference quirks reproduced on request (oracle_set_ref_quirks): bit 1 the
+// NPML auxiliary equation driven by the last element's flux, bit 2 the flux
+// columns elasticFluxes never writes carried over from element to element.
+int g_ref_quirks = 0;
 
 // Carpenter & Kennedy (1994) five-stage fourth-order 2N-storage coefficients.
 const double kRK4A[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
@@ -108,6 +112,11 @@ struct Oracle {
 
   // state of one batch member
   std::vector<R> q, qm, qn, rq, th, thm, thn, arq, aux, auxm, auxn, auxr, resq, resth, resaux, ux, ax;
+  // reference quirks: the flux arrays ftemp, gtemp, htemp of timeloop3D as
+  // the element loop leaves them (the last element's values; columns that
+  // elasticFluxes does not write keep the values of earlier elements), (9, Np)
+  int quirks = 0;
+  std::vector<R> lastF, lastG, lastH;
   // NPML trigger (src/timeloopMod.f90:508-542)
   bool trig = false;
   int tw1 = 10, tw2 = 2, tformula = 0, timecrit = 0;
@@ -350,6 +359,10 @@ struct Oracle {
       auxr.assign(ng * 27, R(0));
       resaux.assign(ng * 27, R(0));
     }
+    // ftemp = gtemp = htemp = 0 once before the time loop (src/timeloopMod.f90:224-226)
+    lastF.assign(size_t(9) * Np, R(0));
+    lastG.assign(size_t(9) * Np, R(0));
+    lastH.assign(size_t(9) * Np, R(0));
   }
 
   // Per-thread scratch for one element.
@@ -384,6 +397,15 @@ struct Oracle {
       H[0 * Np + j] = e2 * q9; H[1 * Np + j] = e2 * q9; H[2 * Np + j] = e1 * q9; H[4 * Np + j] = e3 * q8;
       H[5 * Np + j] = e3 * q7; H[6 * Np + j] = e4 * q6; H[7 * Np + j] = e4 * q5; H[8 * Np + j] = e4 * q3;
     }
+    if (quirks & 2) {
+      // f(:,5), g(:,6), h(:,4) are not written by elasticFluxes
+      // (src/waveMod.f90:37-62): they keep what the previous element left
+      for (int j = 0; j < Np; ++j) {
+        F[4 * Np + j] = lastF[4 * Np + j];
+        G[5 * Np + j] = lastG[5 * Np + j];
+        H[3 * Np + j] = lastH[3 * Np + j];
+      }
+    }
     const bool pml_el = pml && pmlc[e];
     if (pml_el) {
       // F <- (F' + F)/kx (src/timeloopMod.f90:399-405) and the NPML
@@ -397,14 +419,22 @@ struct Oracle {
           const R fp = (*AUX)[size_t(i) * ng + g], gp = (*AUX)[size_t(9 + i) * ng + g],
                   hp = (*AUX)[size_t(18 + i) * ng + g];
           const R f = F[i * Np + j], gg = G[i * Np + j], h = H[i * Np + j];
-          auxr[size_t(i) * ng + g] = -alx * fp - ddx / kx * (fp + f);
-          auxr[size_t(9 + i) * ng + g] = -aly * gp - ddy / ky * (gp + gg);
-          auxr[size_t(18 + i) * ng + g] = -alz * hp - ddz / kz * (hp + h);
+          if (!(quirks & 1)) {
+            auxr[size_t(i) * ng + g] = -alx * fp - ddx / kx * (fp + f);
+            auxr[size_t(9 + i) * ng + g] = -aly * gp - ddy / ky * (gp + gg);
+            auxr[size_t(18 + i) * ng + g] = -alz * hp - ddz / kz * (hp + h);
+          }
           F[i * Np + j] = (fp + f) / kx;
           G[i * Np + j] = (gp + gg) / ky;
           H[i * Np + j] = (hp + h) / kz;
         }
       }
+    }
+    if (quirks) {
+      // what ftemp, gtemp, htemp hold after this element (serial loop)
+      std::copy(F, F + size_t(9) * Np, lastF.begin());
+      std::copy(G, G + size_t(9) * Np, lastG.begin());
+      std::copy(H, H + size_t(9) * Np, lastH.begin());
     }
     // Dx = rx Dr + sx Ds + tx Dt etc., column-major (Dx[k*Np+n] = Dx(n,k))
     const size_t NN = size_t(Np) * Np;
@@ -567,8 +597,35 @@ struct Oracle {
 
   void rhs_all(const std::vector<R>& Q, const std::vector<R>* TH, const std::vector<R>* AUX, int it, int stage,
                int batch) {
+    if (!quirks) {
 #pragma omp parallel for schedule(dynamic, 64)
+      for (int e = 0; e < K; ++e) rhs_element(e, Q, TH, AUX, it, stage, batch);
+      return;
+    }
+    // the reference's order: one element after the other, the flux arrays
+    // carried from each element to the next (src/timeloopMod.f90:395-476)
     for (int e = 0; e < K; ++e) rhs_element(e, Q, TH, AUX, it, stage, batch);
+    if ((quirks & 1) && pml) {
+      // RungeKuttaSteps applies ftemp(j,i) -- the LAST element's flux, modified
+      // when that element is in the PML -- to node j of every PML element
+      // (src/rungekuttaMod.f90:52-63, called at src/timeloopMod.f90:479-480)
+      for (int e = 0; e < K; ++e) {
+        if (!pmlc[e]) continue;
+        for (int j = 0; j < Np; ++j) {
+          const size_t g = size_t(e) * Np + j;
+          const R ddx = prof[g], ddy = prof[ng + g], ddz = prof[2 * ng + g];
+          const R alx = prof[3 * ng + g], aly = prof[4 * ng + g], alz = prof[5 * ng + g];
+          const R kx = prof[6 * ng + g], ky = prof[7 * ng + g], kz = prof[8 * ng + g];
+          for (int i = 0; i < 9; ++i) {
+            const R fp = (*AUX)[size_t(i) * ng + g], gp = (*AUX)[size_t(9 + i) * ng + g],
+                    hp = (*AUX)[size_t(18 + i) * ng + g];
+            auxr[size_t(i) * ng + g] = -alx * fp - ddx / kx * (fp + lastF[size_t(i) * Np + j]);
+            auxr[size_t(9 + i) * ng + g] = -aly * gp - ddy / ky * (gp + lastG[size_t(i) * Np + j]);
+            auxr[size_t(18 + i) * ng + g] = -alz * hp - ddz / kz * (hp + lastH[size_t(i) * Np + j]);
+          }
+        }
+      }
+    }
   }
 
   static R rk2(R a, R an, R dadt, R dt, int irk) {
@@ -692,6 +749,7 @@ template <class R>
 int run_t(const nexd_desc* d, int it_end, float* traces, double* field, const TriggerCfg* tc = nullptr) {
   g_loop_seconds = 0.0;
   Oracle<R> o(*d);
+  o.quirks = g_ref_quirks;
   std::fill(traces, traces + size_t(d->nrec) * d->nt * 9 * std::max(1, d->nbatch), 0.0f);
   const int nb = std::max(1, d->nbatch);
   if (tc) {
@@ -786,6 +844,15 @@ int oracle_rhs(const nexd_desc* d, int precision, int it, int stage, const doubl
 }
 
 double oracle_loop_seconds() { return g_loop_seconds; }
+
+int oracle_set_ref_quirks(int flags) {
+  if (flags < 0 || flags > 3) {
+    g_err = "ref_quirks flags must be 0..3";
+    return NEXD_ERR_INVALID;
+  }
+  g_ref_quirks = flags;
+  return 0;
+}
 
 int oracle_last_error(char* buf, size_t len) {
   if (!buf || !len) return NEXD_ERR_INVALID;

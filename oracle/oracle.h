@@ -50,6 +50,20 @@ int oracle_last_error(char* buf, size_t len);
  * timed region. */
 double oracle_loop_seconds(void);
 
+/* Reproduces two of the reference's quirks in later oracle_run calls (all
+ * threads; 0 restores the default, a correct NPML):
+ *   bit 1  the NPML auxiliary equation of every PML element is driven by the
+ *          flux arrays ftemp/gtemp/htemp as the element loop leaves them, i.e.
+ *          the LAST element's flux (src/rungekuttaMod.f90:52-63 called with
+ *          them at src/timeloopMod.f90:479-480); the default uses each
+ *          element's own flux;
+ *   bit 2  the flux columns elasticFluxes never writes (f(:,5), g(:,6),
+ *          h(:,4), src/waveMod.f90:37-62) keep the values the previous element
+ *          left in them; the default has them zero.
+ * With either bit the element loop runs serially in mesh order, as in the
+ * reference.  Returns 0, or NEXD_ERR_INVALID for flags outside 0..3. */
+int oracle_set_ref_quirks(int flags);
+
 #ifdef __cplusplus
 }
 #endif

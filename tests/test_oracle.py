@@ -8,7 +8,7 @@ import pytest
 
 from conftest import (GOLDEN, brick_dt_cfl, pin_brick_edge_stations, run_oracle, run_oracle_trigger, trace_misfit,
                       station_misfit, write_brick, rel_l2)
-from nexd_b200 import Mesh, synth
+from nexd_b200 import Mesh, _abi, synth
 
 
 @pytest.fixture(scope="module")
@@ -144,3 +144,37 @@ def test_fullrun_fixture_matches_oracle_prefix(tmp_path, oracle, name):
     assert np.allclose(fx.fingerprint(m), ref["fingerprint"], rtol=1e-12, atol=0)
     tr = run_oracle(oracle, m, 64, steps=60)[..., 0]
     assert np.array_equal(tr[:, :60], ref["traces"][:, :60])
+
+
+def test_ref_quirks_switch_reports_the_reference_npml(tmp_path, oracle):
+    """oracle_set_ref_quirks reproduces what the reference computes on the NPML
+    path: bit 1 drives every PML element's auxiliary equation with the last
+    element's flux (src/rungekuttaMod.f90:52-63 with the ftemp/gtemp/htemp the
+    element loop leaves behind), bit 2 carries the flux columns elasticFluxes
+    never writes from element to element (src/waveMod.f90:37-62).  Two-layer
+    anelastic model with a 3-cell NPML around a 4 x 4 x 2-cell interior
+    (3,000 tets), N=2, the reference's RK2 at CFL 0.15, 400 steps: the
+    carried columns change nothing (the auxiliaries of those columns start
+    at zero and stay zero), the last-element flux moves the traces by the
+    deviation printed here, 4.6e-2 (the correct NPML is the default of the
+    oracle and of the GPU path)."""
+    oracle.oracle_set_ref_quirks.argtypes = [C.c_int]
+    d = str(tmp_path / "q")
+    synth.write_twolayer(d, cells=(10, 10, 5), nt=400, nrec=8, src_depth=(700.0, 700.0))
+    m = Mesh(d, N=2, timeint=2, cfl=0.15)  # RK2 at N=2 is unstable at CFL 0.3
+    assert m.array("pmlcheck").sum() > 0
+    base = run_oracle(oracle, m, 64)[..., 0]
+    try:
+        assert oracle.oracle_set_ref_quirks(2) == 0
+        carried = run_oracle(oracle, m, 64)[..., 0]
+        assert oracle.oracle_set_ref_quirks(3) == 0
+        both = run_oracle(oracle, m, 64)[..., 0]
+        assert oracle.oracle_set_ref_quirks(4) == _abi.NEXD_ERR_INVALID
+    finally:
+        oracle.oracle_set_ref_quirks(0)
+    assert np.array_equal(carried, base)
+    assert np.isfinite(both).all()
+    dev = trace_misfit(both, base)
+    print(f"reference NPML (last-element flux) vs correct NPML: trace relative L2 {dev:.3e}")
+    assert 1e-3 < dev < 0.5
+    assert np.abs(both).max() < 10 * np.abs(base).max()  # a different NPML, not a blow-up
