@@ -618,15 +618,6 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   c->ldt = c->ldq;
   c->lda = ((long long)c->Kpml * Np + 63) / 64 * 64;
   const int nb = c->nbatch;
-  // per-element scalars of the stage tail in the record: Zener coefficients,
-  // first source, receiver slot (read from shared memory with the record)
-  for (int ni = 0; ni < K; ++ni) {
-    float* g = &h_geo[size_t(ni) * GEO_STRIDE];
-    if (c->att)
-      for (int j = 0; j < 3 * c->nMB; ++j) g[G_AEL + j] = h_ael[size_t(ni) * 3 * c->nMB + j];
-    std::memcpy(&g[G_SRC], &h_head[ni], sizeof(float));
-    std::memcpy(&g[G_SLOT], &h_recslot_el[ni], sizeof(float));
-  }
   if ((st = upload(c, &c->D, h_D)) || (st = upload(c, &c->L, h_L)) || (st = upload(c, &c->geo, h_geo)) ||
       (st = upload(c, &c->patterns, pat)))
     return fail(st);

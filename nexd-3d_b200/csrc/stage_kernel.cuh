@@ -55,10 +55,10 @@ struct Order {
   static constexpr int SL = 4 * NPAIR * Np * 2; // LIFT as [face][pair][n][2]
   // one prefetch buffer: element records, own wavefield (field-major), the
   // neighbour face traces and the connectivity of the following chunk
-  // element records (80 words) at an 84-word stride: the same field of
-  // the elements that share a warp falls on different banks (84 = 20 mod 32;
-  // an 80-word stride would put elements 0 and 2 on one bank)
-  static constexpr int GSTR = 84;
+  // element records at a 68-word stride: the same field of different
+  // elements in one warp falls on different banks (a 64-word stride puts it
+  // on one bank)
+  static constexpr int GSTR = 68;
   static constexpr int SGEO = E * GSTR;
   // Own wavefield: one slot of QF floats per field holding the chunk's node
   // range [e0 Np, (e0 + ne) Np) widened to 16-byte boundaries (at most E Np
@@ -112,10 +112,7 @@ enum GeoOffset {
   G_IZS = 61,  // 1/(rho vs)
   G_AP = 62,   // 1/(lambda+2mu)
   G_AS = 63,   // 1/(2mu)
-  G_AEL = 64,  // Zener coefficients of mechanism l: -lam Ylam, -2mu Ymu, their sum (64 + 3l ..)
-  G_SRC = 73,  // first source of the element (int bits), -1 for none
-  G_SLOT = 74, // receiver slot of the element (int bits), -1 for none
-  GEO_STRIDE = 80
+  GEO_STRIDE = 64
 };
 
 enum StageMode { MODE_LSERK = 0, MODE_TVD = 1 };
@@ -136,7 +133,7 @@ struct StageArgs {
   int npat;
   const float* ael;    // [K][3*nMB]: -lam*Ylam, -2mu*Ymu, sum (src/timeloopMod.f90:274-282)
   const float* wl;     // [nMB]
-  float wlv[3];        // the relaxation frequencies as kernel parameters
+  float wlv[3];        // the relaxation frequencies w_l as kernel parameters (nMB = 3)
   const float* prof;   // [Kpml][9][Np]: ddx ddy ddz ax ay az kx ky kz
   // state, batch member b at offset b*9*ldq (q/res), b*6*nMB*ldt (theta), b*27*lda (aux)
   const float* q_in;
@@ -384,11 +381,11 @@ struct NodePrefetch {
   float ae[(ATT && EARLY) ? 3 * kNMB : 1];  // per-element Zener coefficients
   int src, slot, pml_off;                   // first source of the element, receiver slot, NPML switched off
 
-  // g: the element's record in shared memory (Zener coefficients, first
-  // source and receiver slot are part of it)
-  __device__ __forceinline__ const float* zener(const float* g) const { return EARLY ? ae : g + G_AEL; }
-  __device__ __forceinline__ int first_source(const float* g) const { return EARLY ? src : __float_as_int(g[G_SRC]); }
-  __device__ __forceinline__ int receiver_slot(const float* g) const { return EARLY ? slot : __float_as_int(g[G_SLOT]); }
+  __device__ __forceinline__ const float* zener(const StageArgs& a, int e) const {
+    return EARLY ? ae : a.ael + (long long)e * 3 * kNMB;
+  }
+  __device__ __forceinline__ int first_source(const StageArgs& a, int e) const { return EARLY ? src : a.src_head[e]; }
+  __device__ __forceinline__ int receiver_slot(const StageArgs& a, int e) const { return EARLY ? slot : a.rec_slot[e]; }
   __device__ __forceinline__ bool npml_off(const StageArgs& a, int b) const { return EARLY ? pml_off != 0 : a.pml_off[b] != 0; }
 
   template <int Np>
@@ -512,12 +509,12 @@ __device__ __forceinline__ void elastic_fluxes(const float* g, const float* qv, 
 template <int Np, bool ATT, bool PML, int MODE, bool EARLY>
 __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, long long node, float* rq, const float* S,
                                             const NodePrefetch<ATT, PML, MODE, EARLY>& p, const float* qown,
-                                            int qstride, const float* g) {
+                                            int qstride) {
   const int n = int(node - (long long)e * Np);
   if (ATT) {
     float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
     float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
-    const float* ae = p.zener(g);
+    const float* ae = p.zener(a, e);
 #pragma unroll
     for (int l = 0; l < kNMB; ++l) {
       const float wl = a.wlv[l];
@@ -548,7 +545,7 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
       }
     }
   }
-  for (int s = p.first_source(g); s >= 0; s = a.src_next[s]) {
+  for (int s = p.first_source(a, e); s >= 0; s = a.src_next[s]) {
     if (a.src_batch[s] != b) continue;
     const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
     const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
@@ -557,7 +554,7 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
     for (int c = 0; c < 9; ++c) rq[c] = fmaf(sp[c * Np], amp, rq[c]);
   }
   if (a.last_stage) {
-    const int slot = p.receiver_slot(g);
+    const int slot = p.receiver_slot(a, e);
     if (slot >= 0) {
       float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
       ab[0] = rq[6];
@@ -880,7 +877,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       S[4] = sig_an[4] - 0.5f * (vgrad[7] + vgrad[5]);
       S[5] = sig_an[5] - 0.5f * (vgrad[6] + vgrad[2]);
     }
-    finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, O::QF, g);
+    finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, O::QF);
   }
   cp_async_wait_all();
 }

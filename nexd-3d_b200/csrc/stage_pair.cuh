@@ -231,10 +231,10 @@ __global__ void __launch_bounds__(256, 1) stage_pair_kernel(const StageArgs a) {
     };
     float S[6];
     if (ATT) strain(sa1, vg1, S);
-    finish_node<Np, ATT, false, MODE>(a, b, e, base + n1, rq1, S, pf1, sQF + le * Np + n1, O::QF, g);
+    finish_node<Np, ATT, false, MODE>(a, b, e, base + n1, rq1, S, pf1, sQF + le * Np + n1, O::QF);
     if (has2) {
       if (ATT) strain(sa2, vg2, S);
-      finish_node<Np, ATT, false, MODE>(a, b, e, base + n2, rq2, S, pf2, sQF + le * Np + n2, O::QF, g);
+      finish_node<Np, ATT, false, MODE>(a, b, e, base + n2, rq2, S, pf2, sQF + le * Np + n2, O::QF);
     }
   }
   cp_async_wait_all();

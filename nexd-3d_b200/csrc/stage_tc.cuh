@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
 
     const bool active = le < ne;
     const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
-    NodePrefetch<ATT, PML, MODE> pf;
+    NodePrefetch<ATT, PML, MODE, true> pf;
     if (active) pf.template load<Np>(a, b, e0 + le, node);
     const int wn = w + gridDim.x;
     Chunk cn;
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
 #pragma unroll
         for (int c = 0; c < 6; ++c) S[c] = r[(9 + c) * T::RS];
       }
-      finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, O::QF, sGeo + le * O::GSTR);
+      finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, O::QF);
     }
   }
   cp_async_wait_all();

@@ -293,10 +293,12 @@ contains
         end if
         st = nexd_destroy(ctx)
 
-! seismograms and energy (src/timeloopMod.f90:591-641); time axis stf(it) = it*deltat
+! seismograms and energy (src/timeloopMod.f90:591-641); the time of step it is
+! (it-1)*deltat, as in the reference's own seismograms (simulations/brick/ref,
+! first row at t = 0)
         allocate(stf_time(par%nt))
         do it = 1, par%nt
-            stf_time(it) = it*deltat
+            stf_time(it) = (it-1)*deltat
         end do
         do r = 1, nrec
             do c = 1, 9

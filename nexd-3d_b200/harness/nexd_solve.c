@@ -50,14 +50,15 @@ static double now_s(void) {
   return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
 }
 
-/* Two-column ASCII time series, one line per step: t_it = it * dt (the
- * reference's stf(it) time axis of the seismograms). */
+/* Two-column ASCII time series, one line per step, step it at (it - 1) dt:
+ * the time axis of the reference's own output files (its seismograms start
+ * at t = 0, simulations/brick/ref/seismo.*). */
 static int write_energy(const char* outdir, const double* energy, int nt, double dt) {
   char path[8192];
   snprintf(path, sizeof path, "%s/energy", outdir);
   FILE* f = fopen(path, "w");
   if (!f) return NEXD_ERR_INVALID;
-  for (int it = 1; it <= nt; ++it) fprintf(f, "%15.7e %15.7e\n", it * dt, energy[it - 1]);
+  for (int it = 1; it <= nt; ++it) fprintf(f, "%15.7e %15.7e\n", (it - 1) * dt, energy[it - 1]);
   fclose(f);
   return NEXD_OK;
 }

@@ -978,6 +978,10 @@ void prepare_solver(MeshDB& db) {
   fill_desc(db);
 }
 
+// Two columns per line, time and value.  The time of step it is (it - 1) dt,
+// as in the reference's own seismograms (simulations/brick/ref/seismo.*,
+// first row at t = 0); the writer in src/timeloopMod.f90:337-339,591-620
+// would label the same rows it*deltat.
 void write_seismograms(const std::string& outdir, const MeshDB& db, const float* traces, int nt, int batch) {
   const int nrec = int(db.rec.size());
   static const char* comp[3] = {"x", "y", "z"};
@@ -993,7 +997,7 @@ void write_seismograms(const std::string& outdir, const MeshDB& db, const float*
         const int ci = k * 3 + c;
         for (int it = 0; it < nt; ++it) {
           const float v = traces[boff + (size_t(ci) * db.par.nt + it) * nrec + r];
-          std::fprintf(f, "   %.8E   %.8E\n", float(double(it + 1) * db.dt), v);
+          std::fprintf(f, "   %.8E   %.8E\n", float(double(it) * db.dt), v);
         }
         std::fclose(f);
       }
