@@ -1969,7 +1969,10 @@ int nexd_get_traces(nexd_ctx* c, float* out) {
 }
 
 namespace {
-// Device layout of a state array: (pointer to batch member b, fields, field stride, elements covered).
+// Device layout of a state array: (pointer to batch member b, fields, field
+// stride, elements covered).  q is field-major ([field][ld]); the memory
+// variables and NPML auxiliaries are element-blocked ([element][field][Np]
+// within the batch member's nf * ld floats).
 int state_view(nexd_ctx* c, int32_t which, int32_t b, float** base, int* nf, long long* ld, int* nel) {
   if (b < 0 || b >= c->nbatch) return set_err(c, NEXD_ERR_INVALID, "batch index out of range");
   if (which == NEXD_STATE_Q) {
@@ -2002,10 +2005,12 @@ int nexd_get_state(nexd_ctx* c, int32_t which, int32_t b, float* out) {
   std::vector<float> h(size_t(nf) * ld);
   CUDA_TRY(c, cudaMemcpyAsync(h.data(), base, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const bool blocked = which != NEXD_STATE_Q;
   for (int f = 0; f < nf; ++f)
     for (int ni = 0; ni < nel; ++ni) {
       const int e = c->new2old[ni];
-      std::memcpy(out + f * nodes + size_t(e) * c->Np, h.data() + f * ld + size_t(ni) * c->Np, c->Np * sizeof(float));
+      const size_t dev = blocked ? (size_t(ni) * nf + f) * c->Np : f * ld + size_t(ni) * c->Np;
+      std::memcpy(out + f * nodes + size_t(e) * c->Np, h.data() + dev, c->Np * sizeof(float));
     }
   return NEXD_OK;
 }
@@ -2023,10 +2028,12 @@ int nexd_set_state(nexd_ctx* c, int32_t which, int32_t b, const float* in) {
     CUDA_TRY(c, cudaMemcpyAsync(h.data(), base, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
+  const bool blocked = which != NEXD_STATE_Q;
   for (int f = 0; f < nf; ++f)
     for (int ni = 0; ni < nel; ++ni) {
       const int e = c->new2old[ni];
-      std::memcpy(h.data() + f * ld + size_t(ni) * c->Np, in + f * nodes + size_t(e) * c->Np, c->Np * sizeof(float));
+      const size_t dev = blocked ? (size_t(ni) * nf + f) * c->Np : f * ld + size_t(ni) * c->Np;
+      std::memcpy(h.data() + dev, in + f * nodes + size_t(e) * c->Np, c->Np * sizeof(float));
     }
   CUDA_TRY(c, cudaMemcpyAsync(base, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));

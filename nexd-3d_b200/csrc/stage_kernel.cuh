@@ -367,6 +367,17 @@ __device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, 
 // Memory variables per mechanism set: the reference's nMB = 3 (src/constants.h:36).
 constexpr int kNMB = 3;
 
+// Element-local state (LSERK residual of q, memory variables and their
+// residuals, NPML auxiliaries and their residuals) is element-blocked: field f
+// of node n of element e of batch member b sits at
+//   b F ld + (e F + f) Np + n,
+// so every field of a node is a compile-time offset from one address (ld >=
+// elements x Np is the per-field length, the batch stride F ld as for q).
+template <int F, int Np>
+__device__ __forceinline__ long long eblock(long long ld, int b, int e, int n) {
+  return (long long)b * F * ld + (long long)e * F * Np + n;
+}
+
 // Update-phase state of one node, loaded into registers when the chunk starts
 // so the loads are in flight while the face, volume and lift terms run.  With
 // EARLY the per-element scalars of the tail (Zener coefficients, first
@@ -400,10 +411,11 @@ struct NodePrefetch {
         for (int j = 0; j < 3 * kNMB; ++j) ae[j] = __ldg(a.ael + (long long)e * 3 * kNMB + j);
       }
     }
+    const int n = int(node - (long long)e * Np);
     if (MODE == MODE_LSERK) {
-      const float* rs = a.res + (long long)b * 9 * a.ldq + node;
+      const float* rs = a.res + eblock<9, Np>(a.ldq, b, e, n);
 #pragma unroll
-      for (int c = 0; c < 9; ++c) res[c] = __ldcs(rs + c * a.ldq);
+      for (int c = 0; c < 9; ++c) res[c] = __ldcs(rs + c * Np);
     } else if (a.ca != 0.f) {
       const float* qn = a.q_n + (long long)b * 9 * a.ldq + node;
 #pragma unroll
@@ -413,22 +425,22 @@ struct NodePrefetch {
       for (int c = 0; c < 9; ++c) res[c] = 0.f;
     }
     if (ATT) {
-      const float* t = a.th + (long long)b * 6 * kNMB * a.ldt + node;
-      const float* t2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
+      const float* t = a.th + eblock<6 * kNMB, Np>(a.ldt, b, e, n);
+      const float* t2 = a.th2 + eblock<6 * kNMB, Np>(a.ldt, b, e, n);
 #pragma unroll
-      for (int j = 0; j < NTH; ++j) th[j] = __ldcs(t + j * a.ldt);
+      for (int j = 0; j < NTH; ++j) th[j] = __ldcs(t + j * Np);
 #pragma unroll
-      for (int j = 0; j < NTH; ++j) th2[j] = need2 ? __ldcs(t2 + j * a.ldt) : 0.f;
+      for (int j = 0; j < NTH; ++j) th2[j] = need2 ? __ldcs(t2 + j * Np) : 0.f;
     }
     if (PML) {
-      const long long pn = node;  // PML elements come first internally, so node index = PML node index
-      const float* x = a.aux + (long long)b * 27 * a.lda + pn;
-      const float* x2 = a.aux2 + (long long)b * 27 * a.lda + pn;
-      const float* p = a.prof + (long long)e * 9 * Np + (node - (long long)e * Np);
+      // PML elements come first internally, so element e is PML element e
+      const float* x = a.aux + eblock<27, Np>(a.lda, b, e, n);
+      const float* x2 = a.aux2 + eblock<27, Np>(a.lda, b, e, n);
+      const float* p = a.prof + (long long)e * 9 * Np + n;
 #pragma unroll
-      for (int i = 0; i < 27; ++i) ax[i] = __ldcs(x + i * a.lda);
+      for (int i = 0; i < 27; ++i) ax[i] = __ldcs(x + i * Np);
 #pragma unroll
-      for (int i = 0; i < 27; ++i) ax2[i] = need2 ? __ldcs(x2 + i * a.lda) : 0.f;
+      for (int i = 0; i < 27; ++i) ax2[i] = need2 ? __ldcs(x2 + i * Np) : 0.f;
 #pragma unroll
       for (int i = 0; i < 9; ++i) pr[i] = __ldg(p + i * Np);
     }
@@ -439,15 +451,15 @@ struct NodePrefetch {
 // src/rungekuttaMod.f90:52-63) and the fluxes the volume term differentiates:
 // X, Y, Z = (F'+F)/kx, (G'+G)/ky, (H'+H)/kz, or F, G, H once the trigger
 // switched the layer off.  F, G, H are overwritten.
-template <bool ATT, int MODE, bool EARLY>
-__device__ __forceinline__ void pml_node(const StageArgs& a, int b, long long pn,
+template <int Np, bool ATT, int MODE, bool EARLY>
+__device__ __forceinline__ void pml_node(const StageArgs& a, int b, int e, int n,
                                          const NodePrefetch<ATT, true, MODE, EARLY>& p, float* F, float* G, float* H) {
   if (p.npml_off(a, b)) return;  // pmlcheck(:) = .false.: ordinary element (src/timeloopMod.f90:537)
   const float ddx = p.pr[0], ddy = p.pr[1], ddz = p.pr[2];
   const float alx = p.pr[3], aly = p.pr[4], alz = p.pr[5];
   const float ikx = 1.f / p.pr[6], iky = 1.f / p.pr[7], ikz = 1.f / p.pr[8];
-  float* aux = a.aux + (long long)b * 27 * a.lda + pn;
-  float* aux2 = a.aux2 + (long long)b * 27 * a.lda + pn;
+  float* aux = a.aux + eblock<27, Np>(a.lda, b, e, n);
+  float* aux2 = a.aux2 + eblock<27, Np>(a.lda, b, e, n);
   const float* av = p.ax;
   const float* a2 = p.ax2;
 #pragma unroll
@@ -462,18 +474,18 @@ __device__ __forceinline__ void pml_node(const StageArgs& a, int b, long long pn
       const float r1 = a.ca * a2[i] + a.dt * rf;
       const float r2 = a.ca * a2[9 + i] + a.dt * rg;
       const float r3 = a.ca * a2[18 + i] + a.dt * rh;
-      __stcs(aux2 + i * a.lda, r1);
-      __stcs(aux2 + (9 + i) * a.lda, r2);
-      __stcs(aux2 + (18 + i) * a.lda, r3);
+      __stcs(aux2 + i * Np, r1);
+      __stcs(aux2 + (9 + i) * Np, r2);
+      __stcs(aux2 + (18 + i) * Np, r3);
       nf = fp + a.cb * r1;
       ng_ = gp + a.cb * r2;
       nh = hp + a.cb * r3;
     } else {
       float n1, n2, n3;
       if (a.stage_first) {
-        __stcs(aux2 + i * a.lda, fp);
-        __stcs(aux2 + (9 + i) * a.lda, gp);
-        __stcs(aux2 + (18 + i) * a.lda, hp);
+        __stcs(aux2 + i * Np, fp);
+        __stcs(aux2 + (9 + i) * Np, gp);
+        __stcs(aux2 + (18 + i) * Np, hp);
         n1 = fp; n2 = gp; n3 = hp;
       } else {
         n1 = a2[i]; n2 = a2[9 + i]; n3 = a2[18 + i];
@@ -482,9 +494,9 @@ __device__ __forceinline__ void pml_node(const StageArgs& a, int b, long long pn
       ng_ = a.ca * n2 + a.cb * (gp + a.dt * rg);
       nh = a.ca * n3 + a.cb * (hp + a.dt * rh);
     }
-    __stcs(aux + i * a.lda, nf);
-    __stcs(aux + (9 + i) * a.lda, ng_);
-    __stcs(aux + (18 + i) * a.lda, nh);
+    __stcs(aux + i * Np, nf);
+    __stcs(aux + (9 + i) * Np, ng_);
+    __stcs(aux + (18 + i) * Np, nh);
     F[i] = phi;
     G[i] = psi;
     H[i] = ome;
@@ -512,8 +524,8 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
                                             int qstride) {
   const int n = int(node - (long long)e * Np);
   if (ATT) {
-    float* th = a.th + (long long)b * 6 * kNMB * a.ldt + node;
-    float* th2 = a.th2 + (long long)b * 6 * kNMB * a.ldt + node;
+    float* th = a.th + eblock<6 * kNMB, Np>(a.ldt, b, e, n);
+    float* th2 = a.th2 + eblock<6 * kNMB, Np>(a.ldt, b, e, n);
     const float* ae = p.zener(a, e);
 #pragma unroll
     for (int l = 0; l < kNMB; ++l) {
@@ -530,7 +542,7 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
         const float r = wl * (S[j] - t[j]);
-        const long long o = (l * 6 + j) * a.ldt;
+        const int o = (l * 6 + j) * Np;
         float nt_;
         if (MODE == MODE_LSERK) {
           const float rr = a.ca * t2[j] + a.dt * r;
@@ -564,11 +576,11 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
   }
   float* qo = a.q_out + (long long)b * 9 * a.ldq + node;
   if (MODE == MODE_LSERK) {
-    float* rs = a.res + (long long)b * 9 * a.ldq + node;
+    float* rs = a.res + eblock<9, Np>(a.ldq, b, e, n);
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
       const float r = a.ca * p.res[c] + a.dt * rq[c];
-      __stcs(rs + c * a.ldq, r);
+      __stcs(rs + c * Np, r);
       __stcs(qo + c * a.ldq, qown[c * qstride] + a.cb * r);
     }
   } else {
@@ -707,7 +719,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
       for (int c = 0; c < 9; ++c) qv[c] = sQF[c * O::QF + le * Np + n];
       float F[9], G[9], H[9];
       elastic_fluxes(g, qv, F, G, H);
-      pml_node<ATT, MODE>(a, b, node, pf, F, G, H);
+      pml_node<Np, ATT, MODE>(a, b, e0 + le, n, pf, F, G, H);
       // the row as 8-byte stores (pairs of fields; field 8 with the zero pad):
       // 16 threads at a 34-word stride touch 32 different banks
       float2* cf = reinterpret_cast<float2*>(sCF + le * O::CFE + n * CS);

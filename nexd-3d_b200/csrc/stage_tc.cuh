@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256, 1) stage_tc_kernel(const StageArgs a, con
       for (int c = 0; c < 9; ++c) qv[c] = sQF[c * O::QF + le * Np + n];
       float F[9], G[9], H[9];
       elastic_fluxes(g, qv, F, G, H);
-      if constexpr (PML) pml_node<ATT, MODE>(a, b, node, pf, F, G, H);
+      if constexpr (PML) pml_node<Np, ATT, MODE>(a, b, e0 + le, n, pf, F, G, H);
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const float m0 = g[G_RX + 3 * d], m1 = g[G_RY + 3 * d], m2 = g[G_RZ + 3 * d];
