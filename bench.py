@@ -19,7 +19,9 @@ Other workloads (measurements beside the headline, not the headline):
   batch64  the two-layer model with 64 independent moment-tensor sources in
            one launch (64 wavefields, ~115 GB of state)
   multimodel  16 seeded models (8k-300k tets, N=2..5, elastic or anelastic)
-           stepped together as one CUDA graph, grids autotuned
+           stepped together as one CUDA graph: one persistent launch per stage
+           for all models or one branch per model, whichever the autotune
+           measures faster
   learned  the two-layer model with its NPML replaced by the learned
            absorbing boundary: the network is trained first (wide-NPML runs
            at 1,536 tets, scored on held-out sources against the wide run,
@@ -147,6 +149,7 @@ def run_multimodel(args, grp, tmp, steps, warmup):
         solvers.append(s)
     g = Group(solvers)
     div = g.autotune()
+    gmode, gblocks, gms = g.mode()
     g.run(1, warmup)
     grp.barrier()
     torch.cuda.synchronize()
@@ -188,7 +191,10 @@ def run_multimodel(args, grp, tmp, steps, warmup):
                    "models": [dict(tets=m.K, N=m.N, anelastic=bool(m.desc.attenuation),
                                    kernel=s.contraction()[0]["rest"]) for m, s in zip(meshes, solvers)],
                    "total_tets": int(sum(m.K for m in meshes)), "integrator": "LSERK4 (5 stages)",
-                   "timed": "one CUDA graph per two steps, one branch per model; grids autotuned",
+                   "timed": "one CUDA graph per two steps; autotuned between one branch per model "
+                            "(grid divisor) and one persistent launch per stage for all models",
+                   "group_mode": "one persistent launch per stage" if gmode == 1 else "one graph branch per model",
+                   "autotune_ms_three_probe_stages": gms, "persistent_blocks_per_model": gblocks,
                    "grid_divisor": div, "l2": "inputs larger than L2",
                    "parallelism": f"replicas x{grp.world}"},
         "roofline": {"bound": "hbm", "kernel": "all stage kernels of the group (step average)", "achieved": achieved,

@@ -250,10 +250,11 @@ typedef struct nexd_profile {
  * NEXD_CONTRACT_AUTO times the candidate kernels on this mesh (a few stage
  * launches at the current step boundary that leave the live state unchanged)
  * and keeps the fastest per element class (NPML elements, the rest): the FP32
- * kernel, the tensor-core kernel (order 4) and, outside the NPML, an FP32
- * kernel with a thread per node pair (orders 2-5; bit-identical to the FP32
- * kernel).  Results of the FP32 and tensor-core kernels agree to FP32
- * rounding, not bit for bit.  NEXD_CONTRACT_AUTO is accepted for every order. */
+ * kernel, the tensor-core kernel (order 4), outside the NPML an FP32 kernel
+ * with a thread per node pair and on NPML elements an FP32 kernel with two
+ * threads per node (orders 2-5; both bit-identical to the FP32 kernel).
+ * Results of the FP32 and tensor-core kernels agree to FP32 rounding, not bit
+ * for bit.  NEXD_CONTRACT_AUTO is accepted for every order. */
 enum nexd_contraction {
   NEXD_CONTRACT_FP32 = 0,
   NEXD_CONTRACT_BF16X3 = 1,
@@ -263,15 +264,17 @@ enum nexd_contraction {
 int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
 
 /* The kernel kind in use per element class (kinds[0] NPML elements, kinds[1]
- * the rest: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3 or 2 = the node-pair FP32
- * kernel) and, after an AUTO selection, the measured ms per stage launch
- * tune_ms[class * 3 + kind] (0 where not measured).  Either pointer may be NULL. */
+ * the rest: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3, 2 = the node-pair FP32
+ * kernel (the rest) or 3 = the FP32 kernel with two threads per node (NPML
+ * elements)) and, after an AUTO selection, the measured ms per stage launch
+ * tune_ms[class * 4 + kind] (8 floats; 0 where not measured).  Either pointer
+ * may be NULL. */
 int nexd_get_contraction(const nexd_ctx* ctx, int32_t* kinds, float* tune_ms);
 
 /* Pins the kernel per element class without timing: kinds[0] for NPML
- * elements (NEXD_CONTRACT_FP32 or NEXD_CONTRACT_BF16X3), kinds[1] for the rest
- * (those two or 2 = the node-pair FP32 kernel), as nexd_get_contraction
- * reports them -- e.g. to replay an earlier AUTO choice, so that repeated or
+ * elements (NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3 or 3 = two threads per
+ * node, orders 2-5), kinds[1] for the rest (the first two or 2 = the
+ * node-pair FP32 kernel), as nexd_get_contraction reports them -- e.g. to replay an earlier AUTO choice, so that repeated or
  * profiled runs use the same kernels.  NEXD_ERR_UNSUPPORTED for a kind the
  * order lacks, NEXD_ERR_INVALID for an unknown kind. */
 int nexd_set_contraction_kinds(nexd_ctx* ctx, const int32_t* kinds);
@@ -345,13 +348,30 @@ int nexd_mlp_adam(int64_t count, float* params, const float* grads, float* m, fl
  * it_begin..it_end of every member (within every member's nt).
  * nexd_group_autotune times harmless first-stage launches of all members
  * running together (they leave the live state unchanged) with the members'
- * persistent grids divided by 1, 2 or 4 and keeps the fastest divisor.
+ * persistent grids divided by 1, 2 or 4 and keeps the fastest divisor, then
+ * compares that with the single persistent launch (mode 1 below).
  * nexd_group_span: device time of the last nexd_group_run (CUDA events). */
 typedef struct nexd_group nexd_group;
 int nexd_group_create(nexd_ctx* const* members, int32_t n, nexd_group** out);
 int nexd_group_run(nexd_group* group, int32_t it_begin, int32_t it_end);
 int nexd_group_autotune(nexd_group* group, int32_t* divisor);
 int nexd_group_span(const nexd_group* group, double* span_ms);
+/* Execution mode of a group.  0: the graph holds one branch per member with
+ * the member's own kernels (as above).  1: every LSERK stage of all members
+ * is ONE persistent launch, whose blocks each work through a share of one
+ * member's (wavefield, element chunk) work items with that member's order
+ * and rheology -- the same per-element arithmetic as the member's FP32
+ * kernel, so results are identical; the blocks are shared out in proportion
+ * to each member's measured stage time.  Mode 1 covers up to 16 members that
+ * step with LSERK4, have orders 2-5 and no NPML elements, energy trigger,
+ * movie or learned boundary, and do not use the tensor-core contraction
+ * (NEXD_ERR_UNSUPPORTED otherwise).  nexd_group_autotune measures both modes
+ * (three probe stages each) and keeps the faster.  nexd_group_get_mode:
+ * the mode, the blocks of each member in mode 1 (blocks may be NULL, else
+ * sized to the member count) and the autotune's times (tune_ms[0] mode 0,
+ * tune_ms[1] mode 1, ms for three probe stages; may be NULL). */
+int nexd_group_set_mode(nexd_group* group, int32_t mode);
+int nexd_group_get_mode(const nexd_group* group, int32_t* mode, int32_t* blocks, double* tune_ms);
 int nexd_group_destroy(nexd_group* group);
 
 /* Timing of nexd_run with CUDA events on the library's stream, counters reset:

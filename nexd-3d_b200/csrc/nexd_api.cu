@@ -19,6 +19,8 @@
 #include "stage_kernel.cuh"
 #include "stage_tc.cuh"
 #include "stage_pair.cuh"
+#include "stage_npml_split.cuh"
+#include "group_kernel.cuh"
 #include "boundary_mlp.cuh"
 
 using namespace nexd_dev;
@@ -108,7 +110,7 @@ struct nexd_ctx {
   int contraction = NEXD_CONTRACT_FP32;
   int grid_div = 1;            // persistent grid divided by this (models sharing the GPU in a group)
   int kind[2] = {NEXD_CONTRACT_FP32, NEXD_CONTRACT_FP32};  // kernel per element class: [0] NPML, [1] the rest
-  float tune_ms[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}; // autotune: [class][kind] ms per launch
+  float tune_ms[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};  // autotune: [class][kind] ms per launch
   uint4* ops_tc = nullptr;     // packed operator of the tensor-core kernels (order 4)
   // learned absorbing boundary: absorbing faces, their ghost states and the MLP
   int nbf = 0;                       // absorbing faces
@@ -306,11 +308,33 @@ KernelFn pick_pair_kernel(int N, bool att, int mode, size_t& smem) {
   }
 }
 
-// Kernel kinds per element class: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3
-// and the node-pair FP32 kernel (same results as NEXD_CONTRACT_FP32, chosen
-// by the autotune only).
+// Kernel kinds per element class: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3,
+// the node-pair FP32 kernel (elements outside the NPML) and the NPML kernel
+// with two threads per node (NPML elements); the last two give the same
+// results as NEXD_CONTRACT_FP32 and are chosen by the autotune or pinned.
 constexpr int KIND_FP32_PAIRS = 2;
-constexpr int NKINDS = 3;
+constexpr int KIND_NPML_SPLIT = 3;
+constexpr int NKINDS = 4;
+
+template <int N>
+KernelFn pick_split(bool att, int mode) {
+  if (mode == MODE_LSERK) return att ? stage_npml_split_kernel<N, true, MODE_LSERK> : stage_npml_split_kernel<N, false, MODE_LSERK>;
+  return att ? stage_npml_split_kernel<N, true, MODE_TVD> : stage_npml_split_kernel<N, false, MODE_TVD>;
+}
+
+// The NPML kernel with two threads per node (512-thread blocks; orders 2-5).
+KernelFn pick_split_kernel(int N, bool att, int mode, size_t& smem) {
+  switch (N) {
+    case 2: smem = size_t(SplitOrder<2>::smem_floats()) * 4; return pick_split<2>(att, mode);
+    case 3: smem = size_t(SplitOrder<3>::smem_floats()) * 4; return pick_split<3>(att, mode);
+    case 4: smem = size_t(SplitOrder<4>::smem_floats()) * 4; return pick_split<4>(att, mode);
+    case 5: smem = size_t(SplitOrder<5>::smem_floats()) * 4; return pick_split<5>(att, mode);
+    default: smem = 0; return nullptr;
+  }
+}
+
+// Threads per block of a kernel kind.
+int kind_threads(int kind) { return kind == KIND_NPML_SPLIT ? 512 : 256; }
 
 int elements_per_chunk(int N) {
   const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
@@ -397,13 +421,15 @@ int configure_launch(nexd_ctx* c) {
     } else if (c->kind[which] == KIND_FP32_PAIRS && !pmlk) {
       fn = reinterpret_cast<const void*>(pick_pair_kernel(c->N, c->att, mode, smem));
       E *= 2;
+    } else if (c->kind[which] == KIND_NPML_SPLIT && pmlk) {
+      fn = reinterpret_cast<const void*>(pick_split_kernel(c->N, c->att, mode, smem));
     } else {
       fn = reinterpret_cast<const void*>(pick_kernel(c->N, c->att, pmlk, mode, smem));
     }
     if (!fn) return set_err(c, NEXD_ERR_UNSUPPORTED, "no stage kernel for this order and contraction");
     CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
-    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem));
+    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kind_threads(c->kind[which]), smem));
     if (per_sm < 1) return set_err(c, NEXD_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
     const int nel = pmlk ? c->Kpml : c->K - c->Kpml;
     const long long work = (long long)((nel + E - 1) / E) * c->nbatch;
@@ -842,6 +868,9 @@ void launch_class(nexd_ctx* c, StageArgs& a, bool pml) {
   } else if (c->kind[cls] == KIND_FP32_PAIRS && !pml) {
     KernelFn f = pick_pair_kernel(c->N, c->att, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);
+  } else if (c->kind[cls] == KIND_NPML_SPLIT && pml) {
+    KernelFn f = pick_split_kernel(c->N, c->att, mode, smem);
+    f<<<grid, 512, sm, c->stream>>>(a);
   } else {
     KernelFn f = pick_kernel(c->N, c->att, pml, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);
@@ -889,6 +918,47 @@ StageArgs base_args(nexd_ctx* c) {
   a.nslot = std::max(1, c->nslot);
   a.pml_off = c->pml_off;
   return a;
+}
+
+// The receiver gather of the current step on `stream` (src/timeloopMod.f90:358-373).
+void enqueue_record(nexd_ctx* c, cudaStream_t stream) {
+  if (c->nrec * c->nbatch == 0) return;
+  RecordArgs r{};
+  r.nrec = c->nrec;
+  r.nbatch = c->nbatch;
+  r.Np = c->Np;
+  r.nt = c->nt;
+  r.ldq = c->ldq;
+  r.recelem = c->recelem;
+  r.recslot = c->recslot_of_rec;
+  r.recInt = c->recInt;
+  r.abuf = c->abuf;
+  r.nslot = std::max(1, c->nslot);
+  r.u = c->u;
+  r.traces = c->traces;
+  r.dt = float(c->dt);
+  r.flag = c->flag;
+  r.it_dev = c->it_dev;
+  r.q = c->qbuf[c->cur];
+  const int threads = 128;
+  const int blocks = (c->nrec * c->nbatch * 32 + threads - 1) / threads;
+  record_kernel<<<blocks, threads, 0, stream>>>(r);
+  ++c->launches;
+}
+
+// Stage arguments of LSERK stage s from the current buffer (the stage writes
+// the other one).
+void lserk_stage_args(nexd_ctx* c, int s, StageArgs& a) {
+  a.stage = s;
+  a.last_stage = (s == c->nstage - 1);
+  a.stage_first = (s == 0);
+  a.ca = float(kRK4A[s]);
+  a.cb = float(kRK4B[s]);
+  a.q_in = c->qbuf[c->cur];
+  a.q_out = c->qbuf[1 - c->cur];
+  a.q_n = nullptr;
+  a.e_begin = c->Kpml;
+  a.e_end = c->K;
 }
 
 void enqueue_body(nexd_ctx* c, int nsteps) {
@@ -1197,9 +1267,11 @@ int time_class(nexd_ctx* c, bool pml, int reps, float& ms) {
   return NEXD_OK;
 }
 
-// Picks, per element class, the faster of the FP32 CUDA-core kernel and the
-// tensor-core kernel on this mesh (both FP32-accurate; results of the two
-// agree to FP32 rounding, not bit for bit).
+// Picks, per element class, the fastest on this mesh of the FP32 CUDA-core
+// kernel, the tensor-core kernel (order 4; FP32-accurate, agrees with the
+// FP32 kernel to FP32 rounding, not bit for bit) and the FP32 variants with
+// the same results: the node-pair kernel outside the NPML, the kernel with
+// two threads per node on NPML elements (orders 2-5).
 int autotune(nexd_ctx* c) {
   if (int st = finish(c)) return st;  // at a step boundary
   for (int cls = 0; cls < 2; ++cls) {
@@ -1209,6 +1281,7 @@ int autotune(nexd_ctx* c) {
     for (int k = 0; k < NKINDS; ++k) {
       if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N)) continue;
       if (k == KIND_FP32_PAIRS && (cls == 0 || c->N < 2 || c->N > 5)) continue;
+      if (k == KIND_NPML_SPLIT && (cls == 1 || c->N < 2 || c->N > 5)) continue;
       c->kind[cls] = k;
       if (int st = configure_launch(c)) return st;
       if (int st = time_class(c, cls == 0, 3, c->tune_ms[cls][k])) return st;
@@ -1257,8 +1330,11 @@ int nexd_set_contraction_kinds(nexd_ctx* c, const int32_t* kinds) {
   if (!c || !kinds) return set_err(c, NEXD_ERR_INVALID, "null argument");
   for (int cls = 0; cls < 2; ++cls) {
     const int k = kinds[cls];
-    if (k != NEXD_CONTRACT_FP32 && k != NEXD_CONTRACT_BF16X3 && !(cls == 1 && k == KIND_FP32_PAIRS))
+    if (k != NEXD_CONTRACT_FP32 && k != NEXD_CONTRACT_BF16X3 && !(cls == 1 && k == KIND_FP32_PAIRS) &&
+        !(cls == 0 && k == KIND_NPML_SPLIT))
       return set_err(c, NEXD_ERR_INVALID, "unknown kernel kind for this element class");
+    if (k == KIND_NPML_SPLIT && (c->N < 2 || c->N > 5))
+      return set_err(c, NEXD_ERR_UNSUPPORTED, "the two-threads-per-node NPML kernel covers orders 2 to 5");
     if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N))
       return set_err(c, NEXD_ERR_UNSUPPORTED, "the tensor-core contraction covers order 4");
     if (k == KIND_FP32_PAIRS && (c->N < 2 || c->N > 5))
@@ -1630,6 +1706,12 @@ struct nexd_group {
   std::vector<int> graph_launches;
   float span_ms = 0.f;
   std::string err;
+  // execution mode: 0 one CUDA-graph branch per member (each member's own
+  // kernels), 1 one persistent launch per stage over all members
+  int mode = 0;
+  std::vector<int> bfirst;  // mode 1: first block of each member, then the grid size
+  size_t gsmem = 0;         // mode 1: dynamic shared memory per block
+  float branch_ms = 0.f, persist_ms = 0.f;  // autotune: three probe stages in each mode
 };
 
 namespace {
@@ -1667,15 +1749,23 @@ int fork_join(nexd_group* g, F body) {
   return NEXD_OK;
 }
 
+void enqueue_group_persistent(nexd_group* g, int nsteps);
+
 int capture_group(nexd_group* g) {
   drop_group_graph(g);
   cudaGraph_t graph = nullptr;
   GCUDA(g, cudaStreamBeginCapture(g->s, cudaStreamCaptureModeThreadLocal));
   std::vector<int64_t> before(g->m.size());
-  int st = fork_join(g, [&](size_t i, nexd_ctx* c) {
-    before[i] = c->launches;
-    enqueue_body(c, 2);
-  });
+  int st = NEXD_OK;
+  if (g->mode == 1) {
+    for (size_t i = 0; i < g->m.size(); ++i) before[i] = g->m[i]->launches;
+    enqueue_group_persistent(g, 2);
+  } else {
+    st = fork_join(g, [&](size_t i, nexd_ctx* c) {
+      before[i] = c->launches;
+      enqueue_body(c, 2);
+    });
+  }
   cudaError_t e = cudaStreamEndCapture(g->s, &graph);
   for (size_t i = 0; i < g->m.size(); ++i) {
     g->graph_launches[i] = int(g->m[i]->launches - before[i]);
@@ -1688,6 +1778,95 @@ int capture_group(nexd_group* g) {
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return gerr(g, NEXD_ERR_CUDA, std::string("group instantiate: ") + cudaGetErrorString(e));
   return NEXD_OK;
+}
+
+// Mode 1 covers groups of at most kGroupMax members that all step with LSERK4
+// and have orders 2-5, no NPML elements, no energy trigger, movie or learned
+// boundary, and an FP32 contraction outside the NPML (the FP32 or the
+// bit-identical node-pair kernel: the persistent launch runs the FP32 body).
+bool persistent_eligible(const nexd_group* g) {
+  if (g->m.size() > size_t(kGroupMax)) return false;
+  for (const nexd_ctx* c : g->m)
+    if (c->timeint != 4 || c->Kpml > 0 || c->N < 2 || c->N > 5 || c->energy_on || c->movie_frame > 0 ||
+        c->mlp_on || c->kind[1] == NEXD_CONTRACT_BF16X3)
+      return false;
+  return true;
+}
+
+// Shared memory of the persistent kernel (the largest order's need) and its
+// blocks per SM.
+int group_kernel_config(nexd_group* g, int* per_sm) {
+  int smax = 0;
+  for (const nexd_ctx* c : g->m) smax = std::max(smax, group_smem_floats(c->N));
+  g->gsmem = size_t(smax) * sizeof(float);
+  const void* fn = reinterpret_cast<const void*>(&group_stage_kernel<MODE_LSERK>);
+  GCUDA(g, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g->gsmem)));
+  GCUDA(g, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, 256, g->gsmem));
+  if (*per_sm < 1) return gerr(g, NEXD_ERR_UNSUPPORTED, "the multi-model stage kernel does not fit on an SM");
+  return NEXD_OK;
+}
+
+// Work items (wavefield, chunk) of a member's stage.
+long long member_work(const nexd_ctx* c) {
+  const int E = elements_per_chunk(c->N);
+  return (long long)((c->K + E - 1) / E) * c->nbatch;
+}
+
+// Blocks of each member in proportion to cost[i] (its stage time when it runs
+// alone on the whole GPU), at least one and at most its work items.
+void share_blocks(nexd_group* g, const std::vector<double>& cost, int total) {
+  const int n = int(g->m.size());
+  double sum = 0.0;
+  for (double x : cost) sum += x;
+  g->bfirst.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    const long long want = std::llround(double(total) * cost[i] / std::max(sum, 1e-30));
+    g->bfirst[i + 1] = g->bfirst[i] + int(std::max<long long>(1, std::min(member_work(g->m[i]), want)));
+  }
+}
+
+// A cost model for mode 1 without measurements: work items x Np^2, anelastic
+// elements half again as expensive.
+std::vector<double> model_cost(const nexd_group* g) {
+  std::vector<double> cost;
+  for (const nexd_ctx* c : g->m) cost.push_back(double(member_work(c)) * c->Np * c->Np * (c->att ? 1.5 : 1.0));
+  return cost;
+}
+
+// One persistent launch of stage `args` for every member, on the group stream.
+void launch_group_stage(nexd_group* g, const std::vector<StageArgs>& args) {
+  GroupStageArgs ga{};
+  const int n = int(g->m.size());
+  ga.nmodel = n;
+  for (int i = 0; i < n; ++i) {
+    ga.m[i] = args[i];
+    ga.order[i] = g->m[i]->N;
+    ga.att[i] = g->m[i]->att ? 1 : 0;
+    ga.bfirst[i] = g->bfirst[i];
+  }
+  ga.bfirst[n] = g->bfirst[n];
+  group_stage_kernel<MODE_LSERK><<<g->bfirst[n], 256, g->gsmem, g->s>>>(ga);
+  ++g->m[0]->launches;  // one launch for the whole group, counted once
+}
+
+// nsteps LSERK4 steps of every member in mode 1: the members' receiver
+// gathers, five persistent stage launches, the members' step counters.
+void enqueue_group_persistent(nexd_group* g, int nsteps) {
+  const int n = int(g->m.size());
+  std::vector<StageArgs> args(n);
+  for (int i = 0; i < n; ++i) args[i] = base_args(g->m[i]);
+  for (int step = 0; step < nsteps; ++step) {
+    for (nexd_ctx* c : g->m) enqueue_record(c, g->s);
+    for (int st = 0; st < 5; ++st) {
+      for (int i = 0; i < n; ++i) lserk_stage_args(g->m[i], st, args[i]);
+      launch_group_stage(g, args);
+      for (nexd_ctx* c : g->m) c->cur = 1 - c->cur;
+    }
+    for (nexd_ctx* c : g->m) {
+      tick_kernel<<<1, 32, 0, g->s>>>(c->it_dev);
+      ++c->launches;
+    }
+  }
 }
 
 // Harmless first-stage launches of every member (as in the contraction autotune).
@@ -1767,8 +1946,13 @@ int nexd_group_run(nexd_group* g, int32_t it_begin, int32_t it_end) {
       for (size_t i = 0; i < g->m.size(); ++i) g->m[i]->launches += g->graph_launches[i];
     }
   }
-  if (n == 1)
-    if (int st = fork_join(g, [&](size_t, nexd_ctx* c) { enqueue_body(c, 1); })) return st;
+  if (n == 1) {
+    if (g->mode == 1) {
+      enqueue_group_persistent(g, 1);
+    } else if (int st = fork_join(g, [&](size_t, nexd_ctx* c) { enqueue_body(c, 1); })) {
+      return st;
+    }
+  }
   GCUDA(g, cudaEventRecord(g->span[1], g->s));
   GCUDA(g, cudaEventSynchronize(g->span[1]));
   GCUDA(g, cudaEventElapsedTime(&g->span_ms, g->span[0], g->span[1]));
@@ -1800,6 +1984,45 @@ int nexd_group_autotune(nexd_group* g, int32_t* divisor) {
       best = cand[k];
     }
   }
+  // mode 1: each member's stage alone on the whole GPU sets its block share;
+  // three probe stages of the persistent launch against the best branch time
+  g->mode = 0;
+  if (persistent_eligible(g)) {
+    std::vector<double> cost;
+    for (nexd_ctx* c : g->m) {
+      c->grid_div = 1;
+      if (int st = configure_launch(c)) return gerr(g, st, c->err);
+      float ms = 0.f;
+      if (int st = time_class(c, false, 3, ms)) return gerr(g, st, c->err);
+      cost.push_back(ms);
+    }
+    int per_sm = 0;
+    if (int st = group_kernel_config(g, &per_sm)) return st;
+    share_blocks(g, cost, per_sm * g->m[0]->nsm);
+    std::vector<StageArgs> args;
+    for (nexd_ctx* c : g->m) {
+      StageArgs a = base_args(c);
+      lserk_stage_args(c, 0, a);
+      a.last_stage = 0;
+      a.ca = 0.f;
+      a.cb = 0.f;  // rewrites only the residuals and the other buffer, as the contraction autotune's probes
+      args.push_back(a);
+      set_step_kernel<<<1, 32, 0, g->s>>>(c->it_dev, 1);
+    }
+    const int64_t l0 = g->m[0]->launches;
+    launch_group_stage(g, args);  // warm-up
+    GCUDA(g, cudaEventRecord(g->span[0], g->s));
+    for (int r = 0; r < 3; ++r) launch_group_stage(g, args);
+    GCUDA(g, cudaEventRecord(g->span[1], g->s));
+    GCUDA(g, cudaEventSynchronize(g->span[1]));
+    GCUDA(g, cudaGetLastError());
+    g->m[0]->launches = l0;
+    float pms = 0.f;
+    GCUDA(g, cudaEventElapsedTime(&pms, g->span[0], g->span[1]));
+    g->persist_ms = pms;
+    g->branch_ms = best_ms;
+    if (pms < best_ms) g->mode = 1;
+  }
   for (nexd_ctx* c : g->m) {
     c->grid_div = best;
     if (int st = configure_launch(c)) return gerr(g, st, c->err);
@@ -1807,6 +2030,36 @@ int nexd_group_autotune(nexd_group* g, int32_t* divisor) {
   }
   drop_group_graph(g);
   if (divisor) *divisor = best;
+  return NEXD_OK;
+}
+
+int nexd_group_set_mode(nexd_group* g, int32_t mode) {
+  if (!g) return set_err(nullptr, NEXD_ERR_INVALID, "null group");
+  if (mode != 0 && mode != 1) return gerr(g, NEXD_ERR_INVALID, "group mode must be 0 or 1");
+  if (mode == 1) {
+    if (!persistent_eligible(g))
+      return gerr(g, NEXD_ERR_UNSUPPORTED,
+                  "one persistent launch covers at most 16 LSERK4 members of orders 2-5 without NPML, energy "
+                  "trigger, movie, learned boundary or tensor-core contraction");
+    int per_sm = 0;
+    if (int st = group_kernel_config(g, &per_sm)) return st;
+    if (g->bfirst.size() != g->m.size() + 1) share_blocks(g, model_cost(g), per_sm * g->m[0]->nsm);
+  }
+  g->mode = mode;
+  drop_group_graph(g);
+  return NEXD_OK;
+}
+
+int nexd_group_get_mode(const nexd_group* g, int32_t* mode, int32_t* blocks, double* tune_ms) {
+  if (!g) return set_err(nullptr, NEXD_ERR_INVALID, "null group");
+  if (mode) *mode = g->mode;
+  if (blocks)
+    for (size_t i = 0; i < g->m.size(); ++i)
+      blocks[i] = g->bfirst.size() == g->m.size() + 1 ? g->bfirst[i + 1] - g->bfirst[i] : 0;
+  if (tune_ms) {
+    tune_ms[0] = g->branch_ms;
+    tune_ms[1] = g->persist_ms;
+  }
   return NEXD_OK;
 }
 

@@ -451,17 +451,17 @@ struct NodePrefetch {
 // src/rungekuttaMod.f90:52-63) and the fluxes the volume term differentiates:
 // X, Y, Z = (F'+F)/kx, (G'+G)/ky, (H'+H)/kz, or F, G, H once the trigger
 // switched the layer off.  F, G, H are overwritten.
-template <int Np, bool ATT, int MODE, bool EARLY>
-__device__ __forceinline__ void pml_node(const StageArgs& a, int b, int e, int n,
-                                         const NodePrefetch<ATT, true, MODE, EARLY>& p, float* F, float* G, float* H) {
-  if (p.npml_off(a, b)) return;  // pmlcheck(:) = .false.: ordinary element (src/timeloopMod.f90:537)
-  const float ddx = p.pr[0], ddy = p.pr[1], ddz = p.pr[2];
-  const float alx = p.pr[3], aly = p.pr[4], alz = p.pr[5];
-  const float ikx = 1.f / p.pr[6], iky = 1.f / p.pr[7], ikz = 1.f / p.pr[8];
+// pr: the node's damping profiles, av / a2: its auxiliaries F', G', H' and
+// their LSERK residuals (TVD: step-start values), as loaded for this stage.
+template <int Np, int MODE>
+__device__ __forceinline__ void pml_update(const StageArgs& a, int b, int e, int n, bool off, const float* pr,
+                                           const float* av, const float* a2, float* F, float* G, float* H) {
+  if (off) return;  // pmlcheck(:) = .false.: ordinary element (src/timeloopMod.f90:537)
+  const float ddx = pr[0], ddy = pr[1], ddz = pr[2];
+  const float alx = pr[3], aly = pr[4], alz = pr[5];
+  const float ikx = 1.f / pr[6], iky = 1.f / pr[7], ikz = 1.f / pr[8];
   float* aux = a.aux + eblock<27, Np>(a.lda, b, e, n);
   float* aux2 = a.aux2 + eblock<27, Np>(a.lda, b, e, n);
-  const float* av = p.ax;
-  const float* a2 = p.ax2;
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     const float fp = av[i], gp = av[9 + i], hp = av[18 + i];
@@ -501,6 +501,12 @@ __device__ __forceinline__ void pml_node(const StageArgs& a, int b, int e, int n
     G[i] = psi;
     H[i] = ome;
   }
+}
+
+template <int Np, bool ATT, int MODE, bool EARLY>
+__device__ __forceinline__ void pml_node(const StageArgs& a, int b, int e, int n,
+                                         const NodePrefetch<ATT, true, MODE, EARLY>& p, float* F, float* G, float* H) {
+  pml_update<Np, MODE>(a, b, e, n, p.npml_off(a, b), p.pr, p.ax, p.ax2, F, G, H);
 }
 
 // elasticFluxes (src/waveMod.f90:29-63) with e1..e4 = -(lambda+2mu), -lambda, -mu, -1/rho.
@@ -592,11 +598,15 @@ __device__ __forceinline__ void finish_node(const StageArgs& a, int b, int e, lo
   }
 }
 
+// One block's share of a stage launch: the work items (wavefield, chunk)
+// w0, w0 + wstep, ... of the launch's element range, with `smem` the block's
+// dynamic shared memory (Order<N>::smem_floats(PML) floats).  stage_kernel
+// runs it with w0 = blockIdx.x, wstep = gridDim.x; the multi-model kernel
+// gives each block a share of one model's items.
 template <int N, bool ATT, bool PML, int MODE>
-__global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs a) {
+__device__ __forceinline__ void stage_body(const StageArgs& a, int w0, int wstep, float* smem) {
   using O = Order<N>;
   constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, QS = O::QS, CS = O::CS;
-  extern __shared__ __align__(16) float smem[];
   float* sD = smem;              // 3*Np*Np: D[d][k][n]
   float* sL = sD + O::SD;        // LIFT in face-node pairs
   float* sBuf = sL + O::SL;      // 2 prefetch buffers
@@ -630,13 +640,13 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     le = tid / Np;
     n = tid - le * Np;
   }
-  int w = blockIdx.x;
+  int w = w0;
   if (w >= nwork) return;
 
   // prologue: connectivity of the first chunk straight from global memory
   {
     const Chunk c0 = chunk_of<E>(a, w, nchunk);
-    const int wn = w + gridDim.x;
+    const int wn = w + wstep;
     Chunk c1;
     if (wn < nwork) c1 = chunk_of<E>(a, wn, nchunk);
     int* ids0 = reinterpret_cast<int*>(sBuf + O::BUF + O::SGEO + O::SQF + O::STR);  // scratch: buffer 1's ids slot
@@ -649,7 +659,7 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     issue_chunk<O>(a, c0, ids0, sBuf, wn < nwork ? &c1 : nullptr, sPat);
   }
 
-  for (int p = 0; w < nwork; w += gridDim.x, p ^= 1) {
+  for (int p = 0; w < nwork; w += wstep, p ^= 1) {
     const Chunk ch = chunk_of<E>(a, w, nchunk);
     const int b = ch.b, e0 = ch.e0, ne = ch.ne;
     float* buf = sBuf + p * O::BUF;
@@ -670,10 +680,10 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     if (active) pf.template load<Np>(a, b, e0 + le, node);
     // ---- start the next chunk's copies ------------------------------------------
     {
-      const int wn = w + gridDim.x;
+      const int wn = w + wstep;
       if (wn < nwork) {
         const Chunk cn = chunk_of<E>(a, wn, nchunk);
-        const int wnn = wn + gridDim.x;
+        const int wnn = wn + wstep;
         Chunk cnn;
         if (wnn < nwork) cnn = chunk_of<E>(a, wnn, nchunk);
         issue_chunk<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, wnn < nwork ? &cnn : nullptr, sPat);
@@ -892,6 +902,12 @@ __global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs
     finish_node<Np, ATT, PML, MODE>(a, b, e, node, rq, S, pf, sQF + le * Np + n, O::QF);
   }
   cp_async_wait_all();
+}
+
+template <int N, bool ATT, bool PML, int MODE>
+__global__ void __launch_bounds__(256, PML ? 1 : 2) stage_kernel(const StageArgs a) {
+  extern __shared__ __align__(16) float smem[];
+  stage_body<N, ATT, PML, MODE>(a, blockIdx.x, gridDim.x, smem);
 }
 
 // Receiver gather: one warp per (batch, receiver) (src/timeloopMod.f90:358-373).

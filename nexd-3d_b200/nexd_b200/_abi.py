@@ -66,7 +66,8 @@ GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "
                "nexd_set_contraction", "nexd_get_contraction", "nexd_set_contraction_kinds", "nexd_boundary_faces", "nexd_set_boundary_mlp",
                "nexd_get_ghost", "nexd_get_face_traces", "nexd_mlp_param_count", "nexd_mlp_workspace_floats",
                "nexd_mlp_forward", "nexd_mlp_loss_grad", "nexd_mlp_adam", "nexd_group_create", "nexd_group_run",
-               "nexd_group_autotune", "nexd_group_span", "nexd_group_destroy", "nexd_movie", "nexd_get_movie",
+               "nexd_group_autotune", "nexd_group_span", "nexd_group_destroy", "nexd_group_set_mode",
+               "nexd_group_get_mode", "nexd_movie", "nexd_get_movie",
                "nexd_wavefield_energy_noalloc", "nexd_profile_enable", "nexd_profile_get",
                "nexd_last_error", "nexd_launch_count", "nexd_destroy"]
 NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_ENERGY, NEXD_K_BOUNDARY, NEXD_K_COUNT = 0, 1, 2, 3, 4, 5
@@ -150,6 +151,8 @@ def gpu_lib():
         lib.nexd_group_run.argtypes = [vp, C.c_int32, C.c_int32]
         lib.nexd_group_autotune.argtypes = [vp, C.POINTER(C.c_int32)]
         lib.nexd_group_span.argtypes = [vp, C.POINTER(C.c_double)]
+        lib.nexd_group_set_mode.argtypes = [vp, C.c_int32]
+        lib.nexd_group_get_mode.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         lib.nexd_group_destroy.argtypes = [vp]
         lib.nexd_movie.argtypes = [vp, C.c_int32, C.c_int32]
         lib.nexd_get_movie.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_int32)]

@@ -176,9 +176,13 @@ def record_pairs(wide_solver, wide_elem, face, steps, npf, every=1):
 class Trainer:
     """Adam on the MSE of normalised exterior states, on the GPU."""
 
-    def __init__(self, nin, params=None, hidden=HIDDEN, batch=4096, lr=1e-3, seed=0):
+    def __init__(self, nin, params=None, hidden=HIDDEN, batch=4096, lr=1e-3, seed=0, group=None):
+        """group: a replicas.Group for data-parallel training (each rank fits
+        its own samples; gradients are averaged over the ranks before every
+        Adam step, so all ranks keep the same parameters); None: one process."""
         import torch
         self.torch = torch
+        self.group = group
         self.nin, self.hidden, self.batch, self.lr = nin, hidden, batch, lr
         lib = _abi.gpu_lib()
         self.lib = lib
@@ -214,14 +218,20 @@ class Trainer:
         g = torch.Generator(device="cuda")
         g.manual_seed(seed)
         hist = []
+        from . import replicas
+        nbatch = n // self.batch
+        if self.group is not None:
+            nbatch = replicas.agree_min(self.group, nbatch)  # the same number of all-reduces on every rank
         for _ in range(epochs):
             perm = torch.randperm(n, device="cuda", generator=g)
             tot = torch.zeros((), device="cuda")
             nb = 0
-            for b0 in range(0, n - self.batch + 1, self.batch):
-                idx = perm[b0:b0 + self.batch]
+            for bi in range(nbatch):
+                idx = perm[bi * self.batch:(bi + 1) * self.batch]
                 xb, yb = xd[idx].contiguous(), yd[idx].contiguous()
                 self.loss_grad(xb, yb)
+                if self.group is not None:
+                    replicas.allreduce_mean(self.group, self.grads)
                 self.step += 1
                 st = self.lib.nexd_mlp_adam(self.count, self._ptr(self.params), self._ptr(self.grads),
                                             self._ptr(self.m), self._ptr(self.v), self.step, self.lr, 0.9, 0.999,

@@ -2,9 +2,12 @@
 
 The time loop shards as independent units (sources, models): every rank
 runs its own replica with its own seeded source, no collective touches the
-data path, and the only collectives are the barrier around the timed region
-and the reductions of the timing (maximum over ranks) and of the work (sum
-over ranks).  At the end of a run the receiver traces of every replica are
+time-stepping data path, and the only collectives there are the barrier
+around the timed region and the reductions of the timing (maximum over
+ranks) and of the work (sum over ranks).  Training the learned boundary's
+network data-parallel is the one exchange step: each rank computes the
+gradient of its own shard of face samples and the ranks average them
+(allreduce_mean) before every identical optimizer step.  At the end of a run the receiver traces of every replica are
 gathered on rank 0 (the reference writes each station's seismograms from the
 rank that holds it, src/timeloopMod.f90:591-656; here every rank holds a whole
 replica).  The process group uses NCCL on GPUs and gloo on CPUs (tests).
@@ -78,6 +81,28 @@ def gather_traces(group, traces):
     if group.rank != 0:
         return None
     return np.stack([p.cpu().numpy() for p in parts])
+
+
+def allreduce_mean(group, tensor):
+    """In-place mean of a tensor over the ranks (data-parallel gradients of the
+    boundary network: NCCL all-reduce on GPUs, gloo on CPUs).  One process:
+    unchanged."""
+    if group.dist is None or group.world == 1:
+        return tensor
+    group.dist.all_reduce(tensor, op=group.dist.ReduceOp.SUM)
+    tensor /= group.world
+    return tensor
+
+
+def agree_min(group, value):
+    """The smallest of an integer over the ranks (so that every rank takes the
+    same number of collective steps)."""
+    if group.dist is None or group.world == 1:
+        return int(value)
+    import torch
+    t = torch.tensor([int(value)], dtype=torch.int64, device=group.device)
+    group.dist.all_reduce(t, op=group.dist.ReduceOp.MIN)
+    return int(t.item())
 
 
 def replica_seed(base, rank):

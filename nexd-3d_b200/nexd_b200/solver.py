@@ -100,9 +100,10 @@ class Solver:
             raise _gpu_error(self._ctx, st)
 
     def set_contraction_kinds(self, npml, rest):
-        """Pins the kernel per element class ("fp32", "bf16x3", "fp32_pairs"
-        for the rest), e.g. an earlier auto choice, without timing."""
-        m = {"fp32": 0, "bf16x3": 1, "fp32_pairs": 2}
+        """Pins the kernel per element class ("fp32", "bf16x3"; "fp32_split"
+        for the NPML elements, "fp32_pairs" for the rest), e.g. an earlier
+        auto choice, without timing."""
+        m = {"fp32": 0, "bf16x3": 1, "fp32_pairs": 2, "fp32_split": 3}
         kinds = (C.c_int32 * 2)(m.get(npml, npml), m.get(rest, rest))
         st = _abi.gpu_lib().nexd_set_contraction_kinds(self._ctx, kinds)
         if st != 0:
@@ -111,13 +112,13 @@ class Solver:
     def contraction(self):
         """({"npml": kind, "rest": kind}, autotune ms per launch {(class, kind): ms})."""
         kinds = (C.c_int32 * 2)()
-        ms = (C.c_float * 6)()
+        ms = (C.c_float * 8)()
         st = _abi.gpu_lib().nexd_get_contraction(self._ctx, kinds, ms)
         if st != 0:
             raise _gpu_error(self._ctx, st)
-        names = {0: "fp32", 1: "bf16x3", 2: "fp32_pairs"}
+        names = {0: "fp32", 1: "bf16x3", 2: "fp32_pairs", 3: "fp32_split"}
         return ({"npml": names[kinds[0]], "rest": names[kinds[1]]},
-                {(cl, names[k]): ms[3 * i + k] for i, cl in enumerate(("npml", "rest")) for k in range(3)})
+                {(cl, names[k]): ms[4 * i + k] for i, cl in enumerate(("npml", "rest")) for k in range(4)})
 
     def boundary_faces(self):
         """(elem, face) 1-based arrays of the absorbing faces in ghost-slot order."""
@@ -246,6 +247,22 @@ class Group:
         if st != 0:
             raise _gpu_error(None, st)
         return d.value
+
+    def set_mode(self, mode):
+        """0: one graph branch per member; 1: one persistent launch per stage for all members."""
+        st = _abi.gpu_lib().nexd_group_set_mode(self._g, int(mode))
+        if st != 0:
+            raise _gpu_error(None, st)
+
+    def mode(self):
+        """(mode, blocks per member in mode 1, autotune ms {"branches": .., "persistent": ..})."""
+        m = C.c_int32()
+        blocks = (C.c_int32 * len(self._members))()
+        ms = (C.c_double * 2)()
+        st = _abi.gpu_lib().nexd_group_get_mode(self._g, C.byref(m), blocks, ms)
+        if st != 0:
+            raise _gpu_error(None, st)
+        return m.value, list(blocks), {"branches": ms[0], "persistent": ms[1]}
 
     def span_ms(self):
         v = C.c_double()

@@ -115,3 +115,82 @@ def test_group_errors(tmp_path, solver_mod):
     with pytest.raises(Exception):
         g.run(1, 31)  # beyond nt
     g.run(1, 2)
+
+
+def _no_pml_models(tmp_path):
+    """Members the single persistent launch covers: orders 2 to 5, elastic and
+    anelastic, no NPML, of different sizes."""
+    out = []
+    d = str(tmp_path / "pc2")
+    synth.write_cube(d, cells=4, nt=30)
+    out.append(Mesh(d, N=2, stf_stage_time=True))
+    d = str(tmp_path / "pt3")
+    synth.write_twolayer(d, cells=(8, 8, 4), nt=30, nrec=4, src_depth=(900.0, 900.0), pml=False)
+    out.append(Mesh(d, N=3, stf_stage_time=True))
+    d = str(tmp_path / "pt4")
+    synth.write_twolayer(d, cells=(10, 10, 5), nt=30, nrec=4, src_depth=(900.0, 900.0), pml=False,
+                         attenuation=False, src_seed=5)
+    out.append(Mesh(d, N=4, stf_stage_time=True))
+    d = str(tmp_path / "pt5")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=30, nrec=4, src_depth=(900.0, 900.0), pml=False, src_seed=9)
+    out.append(Mesh(d, N=5, stf_stage_time=True))
+    return out
+
+
+def test_group_single_persistent_launch_equals_member_runs(tmp_path, solver_mod):
+    """Mode 1: every stage of all members is one launch of the multi-model
+    kernel (blocks shared out over the members' work items).  Fields, memory
+    variables and traces are bit-identical to each member run on its own,
+    over graph-replayed step pairs and a leftover step; a group with an NPML
+    member cannot use the mode."""
+    meshes = _no_pml_models(tmp_path)
+    alone = []
+    for m in meshes:
+        s = solver_mod.Solver(m.desc_ptr)
+        s.run(1, 13)
+        alone.append((s.field(), s.traces()))
+        s.close()
+    members = [solver_mod.Solver(m.desc_ptr) for m in meshes]
+    g = solver_mod.Group(members)
+    g.set_mode(1)
+    mode, blocks, _ = g.mode()
+    assert mode == 1 and all(b >= 1 for b in blocks)
+    l0 = sum(s.launch_count() for s in members)
+    g.run(1, 6)
+    g.run(7, 13)
+    # 13 steps x 5 stages: one launch per stage for the whole group
+    per_step_small = sum(1 + (1 if m.nrec > 0 else 0) for m in meshes)  # tick + record per member
+    assert sum(s.launch_count() for s in members) - l0 == 13 * (5 + per_step_small)
+    for s, (f, t) in zip(members, alone):
+        assert np.array_equal(s.field(), f)
+        assert np.array_equal(s.traces(), t)
+    g.close()
+    d = str(tmp_path / "withpml")
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=10, nrec=2, src_depth=(800.0, 800.0))
+    mp = Mesh(d, N=3, stf_stage_time=True)
+    h = solver_mod.Group([solver_mod.Solver(mp.desc_ptr)])
+    with pytest.raises(Exception):
+        h.set_mode(1)
+
+
+def test_group_autotune_chooses_between_modes(tmp_path, solver_mod, oracle):
+    """The group autotune times the per-member branches (grid divisors 1, 2,
+    4) and the single persistent launch, keeps the faster, and the run goes on
+    bit-identically to the members run alone and within the FP32 tolerance
+    of the oracle."""
+    meshes = _no_pml_models(tmp_path)
+    members = [solver_mod.Solver(m.desc_ptr) for m in meshes]
+    g = solver_mod.Group(members)
+    g.run(1, 4)
+    g.autotune()
+    mode, blocks, ms = g.mode()
+    assert mode in (0, 1) and ms["branches"] > 0 and ms["persistent"] > 0
+    assert (mode == 1) == (ms["persistent"] < ms["branches"])
+    g.run(5, 30)
+    for m, s in zip(meshes, members):
+        r = solver_mod.Solver(m.desc_ptr)
+        r.run(1, 30)
+        assert np.array_equal(s.field(), r.field())
+        to, fo = run_oracle(oracle, m, 64, want_field=True)
+        assert rel_l2(s.field(), fo[..., 0]) < 1e-4
+    g.close()

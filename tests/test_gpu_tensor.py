@@ -169,10 +169,10 @@ def test_autotune_leaves_state_and_picks_valid_kinds(tmp_path, oracle, Solver, t
     for x, y in zip(before, after):
         assert np.array_equal(x, y)
     kinds, ms = s.contraction()
-    assert set(kinds.values()) <= {"fp32", "bf16x3", "fp32_pairs"}
-    assert kinds["npml"] != "fp32_pairs"
+    assert set(kinds.values()) <= {"fp32", "bf16x3", "fp32_pairs", "fp32_split"}
+    assert kinds["npml"] != "fp32_pairs" and kinds["rest"] != "fp32_split"
     # every candidate of each class was timed, the chosen one is the fastest
-    for cl, cands in (("npml", ("fp32", "bf16x3")), ("rest", ("fp32", "bf16x3", "fp32_pairs"))):
+    for cl, cands in (("npml", ("fp32", "bf16x3", "fp32_split")), ("rest", ("fp32", "bf16x3", "fp32_pairs"))):
         assert all(ms[(cl, k)] > 0 for k in cands)
         assert ms[(cl, kinds[cl])] == min(ms[(cl, k)] for k in cands)
     s.run(31, 60)
@@ -234,3 +234,33 @@ def test_pinned_kernel_kinds(tmp_path, oracle, Solver):
         s3.set_contraction_kinds("fp32", "bf16x3")
     assert ei.value.status == _abi.NEXD_ERR_UNSUPPORTED
     s3.run(1, 4)
+
+
+@pytest.mark.parametrize("N,att,timeint", [(2, True, 4), (3, False, 4), (4, True, 4), (4, True, 2), (5, True, 4)])
+def test_npml_split_kernel_is_bit_identical(tmp_path, Solver, N, att, timeint):
+    """The NPML kernel with two threads per node (512-thread blocks, one
+    thread holding the NPML auxiliaries, the other the ordinary update state)
+    performs the FP32 NPML kernel's operations in the same order: identical
+    wavefields, memory variables, NPML auxiliaries and traces; AUTO times it
+    for the NPML class."""
+    d = str(tmp_path / "split")
+    synth.write_twolayer(d, cells=(10, 10, 5), nt=12, nrec=4, src_depth=(900.0, 900.0), attenuation=att)
+    m = Mesh(d, N=N, stf_stage_time=True, timeint=timeint, cfl=0.3 if timeint == 4 else 0.1)
+    assert m.array("pmlcheck").sum() > 0
+    a, b = Solver(m.desc_ptr), Solver(m.desc_ptr)
+    b.set_contraction_kinds("fp32_split", "fp32")
+    assert b.contraction()[0] == {"npml": "fp32_split", "rest": "fp32"}
+    a.run(1, 12)
+    b.run(1, 12)
+    assert np.array_equal(a.field(), b.field())
+    if att:
+        nth = 6 * m.desc.nMB
+        assert np.array_equal(a.state(_abi.NEXD_STATE_THETA, nfields=nth), b.state(_abi.NEXD_STATE_THETA, nfields=nth))
+    assert np.array_equal(a.state(_abi.NEXD_STATE_PML, nfields=27), b.state(_abi.NEXD_STATE_PML, nfields=27))
+    assert np.array_equal(a.traces(), b.traces())
+    if N == 4 and timeint == 4:
+        c = Solver(m.desc_ptr)
+        c.set_contraction("auto")
+        kinds, ms = c.contraction()
+        assert ms[("npml", "fp32_split")] > 0 and ms[("npml", "fp32")] > 0
+        assert kinds["npml"] in ("fp32", "bf16x3", "fp32_split")

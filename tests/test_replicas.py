@@ -21,6 +21,7 @@ def _free_port():
 
 
 def _rank_main(rank, world, port, out_dir):
+    import torch
     sys.path.insert(0, PKG)
     os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
                       MASTER_PORT=str(port))
@@ -38,6 +39,12 @@ def _rank_main(rank, world, port, out_dir):
     traces = np.full((2, 5, 9, 1), float(rank + 1), dtype=np.float32, order="F")
     traces[0, :, 0, 0] = np.arange(5) + 10 * rank
     gathered = replicas.gather_traces(g, traces)
+    # data-parallel network training: gradients averaged over the ranks, and
+    # the ranks agree on the number of steps (the smaller shard decides)
+    grads = torch.full((5,), float(rank + 1))
+    replicas.allreduce_mean(g, grads)
+    steps = replicas.agree_min(g, 10 + 3 * rank)
+    np.save(os.path.join(out_dir, f"grad{rank}.npy"), np.append(grads.numpy(), steps))
     g.barrier()
     g.close()
     if rank == 0:
@@ -58,6 +65,9 @@ def test_two_gloo_ranks(tmp_path):
     assert r0[0] == 2.0 and r0[1] == 300.0 and np.isclose(r0[2], 150.0)
     # each rank's replica has its own seeded source
     assert open(tmp_path / "src0.txt").read() != open(tmp_path / "src1.txt").read()
+    for r in range(world):
+        gr = np.load(tmp_path / f"grad{r}.npy")
+        assert np.allclose(gr[:5], 1.5) and gr[5] == 10
     # rank 0 holds every replica's traces in rank order
     gathered = np.load(tmp_path / "gathered.npy")
     assert gathered.shape == (2, 2, 5, 9, 1)
