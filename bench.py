@@ -9,7 +9,7 @@ receivers, LSERK4), synthetic and seeded.  A step is one LSERK4 time step
 fields count).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload twolayer|cube|batch64|multimodel|learned]
+                  [--workload twolayer|cube|batch64|multimodel|learned|partitions]
                   [--contraction fp32|bf16x3|auto|fp32_pairs]
                   [--kernels npml=KIND,rest=KIND]   (pinned per-class kernels)
 
@@ -22,6 +22,9 @@ Other workloads (measurements beside the headline, not the headline):
            stepped together as one CUDA graph: one persistent launch per stage
            for all models or one branch per model, whichever the autotune
            measures faster
+  partitions  the two-layer model split into --parts partitions (coordinate
+           bisection) on one GPU with the per-stage halo exchange of a
+           domain-decomposed run (the reference's SendRecVar)
   learned  the two-layer model with its NPML replaced by the learned
            absorbing boundary: the network is trained first (wide-NPML runs
            at 1,536 tets, scored on held-out sources against the wide run,
@@ -66,6 +69,8 @@ WORKLOADS = {
                     nt=2000, nsrc=64),
     "multimodel": dict(name="16_models_8k_to_300k_tets_N2_to_5_one_graph", cells=None, N=None, nt=1500),
     "learned": dict(name="twolayer_anelastic_learned_boundary_192k_tets_N4_lserk4", cells=(40, 40, 20), N=4, nt=3000),
+    "partitions": dict(name="twolayer_anelastic_npml_192k_tets_N4_lserk4_partitions", cells=(40, 40, 20), N=4,
+                       nt=3000),
 }
 
 
@@ -115,6 +120,64 @@ def train_learned_boundary(tmp, n_train=16, n_eval=4, seed=11, max_reflection=0.
                                          "60/80/100 % of the run and the held-out cases",
                "reference_solution": "8-element NPML around the model (the method itself)"}
     return params, summary
+
+
+def run_partitions(args, grp, tmp, steps, warmup, cells, workload):
+    """The headline model split into --parts partitions (recursive coordinate
+    bisection) on this GPU, stepped together with the per-stage halo exchange
+    (nexd_halo_run).  Reports the whole-mesh rate and the halo kernels' share;
+    on one GPU the halo writes go to this GPU's memory, on several they would
+    cross NVLink (bytes per stage reported for that)."""
+    import torch
+    from nexd_b200.halo import Partitions, PartitionedSolver, element_centroids
+    torch.cuda.set_device(0)
+    wl = WORKLOADS["partitions"]
+    d = os.path.join(tmp, "model")
+    synth.write_twolayer(d, cells=cells, nt=wl["nt"], nrec=100, nsrc=1, src_seed=replicas.replica_seed(2, 0))
+    mesh = Mesh(d, N=wl["N"], stf_stage_time=True)
+    ps = Partitions(mesh.desc_ptr, args.parts, centroids=element_centroids(mesh))
+    p = PartitionedSolver(ps, nrec_total=mesh.nrec)
+    p0 = p.solvers[0]
+    p.run(1, warmup)
+    torch.cuda.synchronize()
+    clk_file = os.path.join(tmp, "clocks.csv")
+    clk = sample_clocks(None, clk_file)
+    time.sleep(0.3)
+    l0 = sum(x.launch_count() for x in p.solvers)
+    p0.profile("span")
+    p.run(warmup + 1, warmup + steps)
+    span = p0.profile()["span_ms"]
+    launches = sum(x.launch_count() for x in p.solvers) - l0
+    for x in p.solvers:
+        x.profile(True)
+    p.run(warmup + steps + 1, warmup + 2 * steps)
+    profs = [x.profile() for x in p.solvers]
+    for x in p.solvers:
+        x.profile(False)
+    clk.terminate()
+    clk.wait()
+    hbytes = p.halo_bytes()
+    kinds = {k: {"launches": sum(q[k]["launches"] for q in profs), "ms": round(sum(q[k]["ms"] for q in profs), 3)}
+             for k in ("record", "stage_pml", "stage_main", "halo")}
+    units = 9 * mesh.Np * mesh.K * 5 * steps
+    halo_ms_stage = kinds["halo"]["ms"] / (5 * steps)
+    line = {
+        "metric": "DOF-stage updates/s", "value": units / (span * 1e-3), "unit": "DOF-stage/s", "n_gpus": 1,
+        "steps": steps, "warmup": warmup, "ms_per_step": span / steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded two-layer model, seeded source)",
+        "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "partitions": args.parts,
+                   "partition_tets": [x.K for x in p.solvers], "integrator": "LSERK4 (5 stages)",
+                   "timed": "partitions interleaved stage by stage in one stream, launched kernel by kernel"},
+        "halo": {"bytes_per_stage": hbytes, "ms_per_stage": halo_ms_stage,
+                 "share_of_step": kinds["halo"]["ms"] / max(1e-9, sum(v["ms"] for v in kinds.values())),
+                 "nvlink_us_per_stage_at_770GBps": hbytes / 770e9 * 1e6},
+        "kernels": kinds, "gpu_launches": int(launches),
+        "clocks": summarize_clocks(clk_file, 0),
+    }
+    p.close()
+    ps.close()
+    print(json.dumps(line), flush=True)
 
 
 def multimodel_specs(seed=4, n=16):
@@ -325,6 +388,7 @@ def main():
     ap.add_argument("--lb-train", type=int, default=16, help="learned workload: training source/material pairs")
     ap.add_argument("--lb-eval", type=int, default=4, help="learned workload: held-out pairs scored")
     ap.add_argument("--lb-epochs", type=int, default=30, help="learned workload: training epochs")
+    ap.add_argument("--parts", type=int, default=2, help="partitions workload: number of partitions")
     ap.add_argument("--cells", default=None, help="hexahedra per axis of the two-layer box (profiling runs use 20,20,10)")
     args = ap.parse_args()
     grp = replicas.init()
@@ -338,6 +402,15 @@ def main():
         tmp = tempfile.mkdtemp(prefix=f"nexd_bench_{rank}_")
         try:
             run_multimodel(args, grp, tmp, steps, warmup)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+            grp.close()
+        return
+    if args.workload == "partitions" and args.impl == "ours":
+        tmp = tempfile.mkdtemp(prefix=f"nexd_bench_{rank}_")
+        try:
+            if rank == 0:
+                run_partitions(args, grp, tmp, args.steps, max(3, args.warmup), cells, workload)
         finally:
             shutil.rmtree(tmp, ignore_errors=True)
             grp.close()

@@ -40,8 +40,12 @@ enum nexd_status {
   NEXD_ERR_NOMEM = 3,       /* device allocation failed */
   NEXD_ERR_UNSUPPORTED = 4, /* valid but not supported by this build (e.g. order) */
   NEXD_ERR_NONFINITE = 5,   /* NaN/Inf detected in the wavefield */
-  NEXD_ERR_NODEVICE = 6     /* no CUDA device visible */
+  NEXD_ERR_NODEVICE = 6,    /* no CUDA device visible */
+  NEXD_ERR_TIMEOUT = 7      /* a halo arrival wait ran out (a peer partition stopped) */
 };
+
+/* Face code of a face shared with another partition (nexd_desc.face). */
+#define NEXD_FACE_PARTITION (-3)
 
 /* Time integrators: 1..3 are the reference's `timeint` values
  * (src/timeloopMod.f90:230-248, src/rungekuttaMod.f90:27-120); 4 is the
@@ -93,9 +97,12 @@ typedef struct nexd_desc {
   const double* ymu;     /* (nMB,K) */
   const double* wl;      /* (nMB) relaxation frequencies */
 
-  /* Connectivity (single partition: mpi_* arrays are not needed). */
-  const int32_t* neighbor; /* (4,K), 0 on a domain boundary */
-  const int32_t* face;     /* (4,K): neighbour's face 1..4, -1 free, -2 absorbing */
+  /* Connectivity.  A face shared with another partition (the reference's
+   * neighbor == -1 with mpi_interface set, src/meshMod.f90:768-790) has
+   * neighbor 0 and face NEXD_FACE_PARTITION; its exterior trace comes from
+   * the halo (nexd_create_partition). */
+  const int32_t* neighbor; /* (4,K), 0 on a domain or partition boundary */
+  const int32_t* face;     /* (4,K): neighbour's face 1..4, -1 free, -2 absorbing, -3 partition */
   const int32_t* ibn;      /* (NpF,4,K): neighbour's node id (global 1-based) matching
                               face node i of this element (src/meshMod.f90:939-987) */
 
@@ -228,7 +235,8 @@ enum nexd_kernel_kind {
   NEXD_K_STAGE_MAIN = 2,
   NEXD_K_ENERGY = 3,
   NEXD_K_BOUNDARY = 4,  /* learned-boundary ghost states */
-  NEXD_K_COUNT = 5
+  NEXD_K_HALO = 5,      /* partition halo writes and arrival waits */
+  NEXD_K_COUNT = 6
 };
 
 typedef struct nexd_profile {
@@ -373,6 +381,90 @@ int nexd_group_span(const nexd_group* group, double* span_ms);
 int nexd_group_set_mode(nexd_group* group, int32_t mode);
 int nexd_group_get_mode(const nexd_group* group, int32_t* mode, int32_t* blocks, double* tune_ms);
 int nexd_group_destroy(nexd_group* group);
+
+/* ---- Partitions and the halo exchange (replaces SendRecVar, src/mpiMod.f90:310-351) ----
+ * A mesh split into partitions runs one context per partition (one process
+ * and GPU per partition, or several partitions of one process on one GPU).
+ * The halo descriptor restates the reference's interface arrays of the
+ * partition (src/meshMod.f90:1006-1110): the neighbour partitions
+ * (mpi_neighbor), per neighbour the shared faces in connection order
+ * (mpi_connection), and per face the index of the same face in the
+ * neighbour's list (mpi_ibool) and the node matching (mpi_ibt).
+ *
+ * Each stage, before its element loop, every partition writes the face
+ * traces of its interface faces straight into the halo slots of its
+ * neighbours' wavefield (peer stores over NVLink, or plain stores when the
+ * neighbour lives on the same GPU), then raises an arrival counter in the
+ * neighbour's memory; the neighbour's stage starts once every neighbour's
+ * counter has arrived (a bounded wait: NEXD_ERR_TIMEOUT after 5 s by default).  The
+ * stage kernels read a halo slot like any neighbour element, so a
+ * partitioned run gives results identical to the whole mesh in one context.
+ * The NPML energy trigger needs a sum over partitions and is not supported
+ * on partitions (NEXD_ERR_UNSUPPORTED). */
+typedef struct nexd_halo_desc {
+  int32_t partition;           /* this partition's number, 1-based (myrank + 1) */
+  int32_t npeer;               /* neighbour partitions (mpi_nn) */
+  const int32_t* peer;         /* (npeer) their partition numbers, 1-based (mpi_neighbor) */
+  const int32_t* nface;        /* (npeer) faces shared with each neighbour (mpi_ninterface) */
+  const int32_t* elem;         /* (sum nface) 1-based element of each shared face, grouped by
+                                  neighbour in connection order (mpi_connection(:,:,1)) */
+  const int32_t* side;         /* (sum nface) its face 1..4 (mpi_connection(:,:,2)) */
+  const int32_t* peer_index;   /* (sum nface) 1-based index of the same face in the
+                                  neighbour's list for this partition (mpi_ibool) */
+  const int32_t* peer_node;    /* (NpF, sum nface) 1-based position, in the neighbour's
+                                  face-node order, of the node matching face node j of
+                                  this partition's face (mpi_ibt) */
+} nexd_halo_desc;
+
+/* nexd_create for one partition: desc describes the partition's own
+ * elements (faces shared with neighbours coded NEXD_FACE_PARTITION) and halo
+ * its interface.  Every NEXD_FACE_PARTITION face must appear exactly once in
+ * halo.  The context runs only after nexd_halo_connect has linked it to
+ * every neighbour. */
+int nexd_create_partition(const nexd_desc* desc, const nexd_halo_desc* halo, nexd_ctx** out);
+
+/* What a neighbour needs to write into this partition: exported by the
+ * receiving partition for its neighbour `peer` (0-based index into
+ * halo.peer), handed to that neighbour's process as bytes (MPI_Alltoall,
+ * torch.distributed), and passed there to nexd_halo_connect. */
+typedef struct nexd_halo_export {
+  int32_t abi_version;       /* NEXD_ABI_VERSION */
+  int32_t device;            /* CUDA device of the exporting context */
+  int64_t pid;               /* exporting process id */
+  int32_t partition;         /* exporting partition, 1-based (as in the neighbour's halo.peer) */
+  int32_t nface;             /* faces shared with the importer */
+  int32_t nbatch;
+  int32_t nbuf;              /* wavefield buffers (2, or 3 for RK3) */
+  int64_t ldq;               /* field stride of the wavefield buffers (floats) */
+  int64_t halo_base;         /* node index of the first halo slot for the importer */
+  int32_t counter_slot;      /* the importer's arrival counter in the exporter */
+  int32_t reserved;
+  uint64_t q[3];             /* device addresses, valid in the exporting process */
+  uint64_t counters;         /* device address of the arrival counters (uint64 each) */
+  unsigned char q_ipc[3][64];    /* cudaIpcMemHandle_t of each buffer (zero when unavailable) */
+  unsigned char counters_ipc[64];
+} nexd_halo_export;
+
+int nexd_halo_export_peer(nexd_ctx* ctx, int32_t peer, nexd_halo_export* out);
+/* Links this partition to its neighbour `peer` (0-based) from that
+ * neighbour's export.  An export from the same process uses its device
+ * addresses directly; one from another process is opened through CUDA IPC.
+ * Resets the arrival counters of the pair. */
+int nexd_halo_connect(nexd_ctx* ctx, int32_t peer, const nexd_halo_export* in);
+
+/* Runs steps it_begin..it_end of n partitions that live in this process on
+ * the current GPU, stage by stage in one stream: every partition's halo
+ * writes of a stage, then every partition's stage (each arrival wait is met
+ * when it starts).  Traces stay in each partition's context.  With
+ * profiling on (nexd_profile_enable) the run span is booked to parts[0] and
+ * each partition's launches to its own counters. */
+int nexd_halo_run(nexd_ctx* const* parts, int32_t n, int32_t it_begin, int32_t it_end);
+
+/* Limit of each arrival wait, in seconds (default 5, at most 60). */
+int nexd_halo_set_timeout(nexd_ctx* ctx, double seconds);
+
+/* Halo bytes written per stage (all neighbours, all wavefields). */
+int nexd_halo_bytes(const nexd_ctx* ctx, int64_t* bytes_per_stage);
 
 /* Timing of nexd_run with CUDA events on the library's stream, counters reset:
  * on = 0 off; 1 per-launch events per kernel kind plus the run span (steps are

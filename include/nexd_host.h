@@ -80,6 +80,35 @@ int nexd_mesh_get_info(const nexd_mesh* mesh, nexd_mesh_info* out);
 int nexd_mesh_write_seismograms(const nexd_mesh* mesh, const char* outdir, const float* traces,
                                 int32_t nt_written, int32_t batch);
 
+/* ---- Partitions: the mesher's domain decomposition for nproc > 1 ------------
+ * The reference's mesher partitions the elements with METIS and hands every
+ * rank its elements and the interface arrays (src/meshMod.f90:382-504,
+ * 669-1110).  nexd_partition_create splits a descriptor into `nparts`
+ * partition descriptors, each with the halo descriptor nexd_create_partition
+ * takes: `part` (K values, 0-based) gives each element's partition (a METIS
+ * result, for instance) or, when NULL, the elements are split by recursive
+ * coordinate bisection of the centroids `centroid` (3,K) into parts whose
+ * sizes differ by at most one.  Partition descriptors keep the elements,
+ * sources and receivers in their original order and share the operators with
+ * `desc`, which must outlive the partition set. */
+typedef struct nexd_partition nexd_partition;
+typedef struct nexd_part_view {
+  const nexd_desc* desc;
+  const nexd_halo_desc* halo;
+  int32_t nelem;
+  const int32_t* elem_global; /* (nelem) 1-based element in the whole mesh */
+  int32_t nsrc;
+  const int32_t* src_global;  /* (nsrc) 1-based source in the whole mesh */
+  int32_t nrec;
+  const int32_t* rec_global;  /* (nrec) 1-based receiver in the whole mesh */
+} nexd_part_view;
+int nexd_partition_create(const nexd_desc* desc, int32_t nparts, const int32_t* part, const double* centroid,
+                          nexd_partition** out);
+/* View of partition `index` (0-based); valid until nexd_partition_free. */
+int nexd_partition_get(const nexd_partition* parts, int32_t index, nexd_part_view* out);
+int nexd_partition_count(const nexd_partition* parts, int32_t* nparts);
+void nexd_partition_free(nexd_partition* parts);
+
 /* Message of the last failed call on this thread. */
 int nexd_mesh_last_error(char* buf, size_t len);
 

@@ -1,6 +1,7 @@
 // C-ABI of libnexd.so (include/nexd.h): device set-up and the time loop.
 //
-// Replaces timeloop3D (src/timeloopMod.f90:42-674) for a single partition.
+// Replaces timeloop3D (src/timeloopMod.f90:42-674) for one partition (the
+// whole mesh, or one part of it with a halo exchange, halo.cuh).
 // Host work here is set-up only (FP64 -> FP32 element records, connectivity
 // patterns, source patterns); every time step runs on the device.
 #include <cuda_runtime.h>
@@ -22,6 +23,9 @@
 #include "stage_npml_split.cuh"
 #include "group_kernel.cuh"
 #include "boundary_mlp.cuh"
+#include "halo.cuh"
+
+#include <unistd.h>
 
 using namespace nexd_dev;
 
@@ -131,6 +135,22 @@ struct nexd_ctx {
   int* gather_idx = nullptr;         // face-trace gather scratch
   float* gather_out = nullptr;
   int gather_cap = 0;
+  // partition halo (nexd_create_partition): halo slots are elements K .. K + nhalo - 1
+  int partition = 0;                 // 1-based partition number, 0 for a whole mesh
+  int nhalo = 0;
+  int npeer = 0;
+  std::vector<int> peer_part, peer_nface, peer_goff;  // per neighbour: number, shared faces, first halo slot
+  std::vector<HaloPeer> peers_h;     // writer's view of each neighbour (filled by nexd_halo_connect)
+  std::vector<char> peer_linked;
+  HaloPeer* peers_dev = nullptr;
+  int* halo_src = nullptr;           // [entries] own node of each shared face node
+  int* halo_dst = nullptr;           // [entries] node offset in the neighbour's halo
+  int* halo_blocks = nullptr;        // [npeer] write blocks each neighbour sends per stage
+  unsigned long long* halo_counters = nullptr;  // [npeer] arrivals from each neighbour
+  unsigned long long* halo_expected = nullptr;  // [npeer] arrivals consumed
+  int put_blocks = 0;
+  unsigned long long halo_limit_ns = 5000000000ull;  // longest arrival wait
+  std::vector<void*> ipc_opened;     // neighbours' buffers opened through CUDA IPC
 };
 
 namespace {
@@ -341,7 +361,7 @@ int elements_per_chunk(int N) {
   return 256 / Np;
 }
 
-int validate(const nexd_desc* d) {
+int validate(const nexd_desc* d, bool partition_ok = false) {
   if (!d) return set_err(nullptr, NEXD_ERR_INVALID, "null descriptor");
   if (d->abi_version != NEXD_ABI_VERSION) return set_err(nullptr, NEXD_ERR_INVALID, "ABI version mismatch");
   if (d->N < 1 || d->N > 5)
@@ -386,7 +406,9 @@ int validate(const nexd_desc* d) {
     for (int f = 0; f < 4; ++f) {
       const int nb = d->neighbor[4 * e + f], fc = d->face[4 * e + f];
       if (nb < 0 || nb > d->nelem) return set_err(nullptr, NEXD_ERR_INVALID, "neighbor index out of range");
-      if (nb == 0 && fc != -1 && fc != -2)
+      if (nb == 0 && fc == NEXD_FACE_PARTITION && !partition_ok)
+        return set_err(nullptr, NEXD_ERR_INVALID, "face shared with another partition (-3) needs nexd_create_partition");
+      if (nb == 0 && fc != -1 && fc != -2 && fc != NEXD_FACE_PARTITION)
         return set_err(nullptr, NEXD_ERR_INVALID, "boundary face that is neither free (-1) nor absorbing (-2)");
       if (nb > 0 && (fc < 1 || fc > 4)) return set_err(nullptr, NEXD_ERR_INVALID, "interior face without neighbour face id");
       if (nb > 0)
@@ -400,6 +422,59 @@ int validate(const nexd_desc* d) {
     if (!(d->rho[e] > 0.0) || !(d->vpu[e] > 0.0) || !(d->vsu[e] > 0.0))
       return set_err(nullptr, NEXD_ERR_INVALID, "non-positive material value");
   }
+  return NEXD_OK;
+}
+
+// The halo descriptor against its partition's descriptor (which passed
+// validate): every shared face listed once, coded as shared in desc, with an
+// index into the neighbour's list and a node matching that are permutations.
+int validate_halo(const nexd_desc* d, const nexd_halo_desc* h) {
+  if (!h) return set_err(nullptr, NEXD_ERR_INVALID, "null halo descriptor");
+  if (h->partition < 1) return set_err(nullptr, NEXD_ERR_INVALID, "partition number must be >= 1");
+  if (h->npeer < 0 || h->npeer > kHaloMaxPeers)
+    return set_err(nullptr, NEXD_ERR_INVALID, "halo: neighbour count out of 0..64");
+  if (h->npeer > 0 && (!h->peer || !h->nface || !h->elem || !h->side || !h->peer_index || !h->peer_node))
+    return set_err(nullptr, NEXD_ERR_INVALID, "halo descriptor has a null array");
+  const int K = d->nelem, NpF = d->NpF;
+  long long total = 0;
+  for (int p = 0; p < h->npeer; ++p) {
+    if (h->peer[p] < 1 || h->peer[p] == h->partition)
+      return set_err(nullptr, NEXD_ERR_INVALID, "halo: neighbour partition number invalid");
+    for (int q = 0; q < p; ++q)
+      if (h->peer[q] == h->peer[p]) return set_err(nullptr, NEXD_ERR_INVALID, "halo: neighbour listed twice");
+    if (h->nface[p] < 1) return set_err(nullptr, NEXD_ERR_INVALID, "halo: neighbour without shared faces");
+    total += h->nface[p];
+  }
+  if (total > 4LL * K) return set_err(nullptr, NEXD_ERR_INVALID, "halo: more shared faces than element faces");
+  std::vector<char> seen(size_t(4) * K, 0);
+  std::vector<char> used;
+  long long i = 0;
+  for (int p = 0; p < h->npeer; ++p) {
+    used.assign(size_t(h->nface[p]), 0);
+    for (int c = 0; c < h->nface[p]; ++c, ++i) {
+      const int e = h->elem[i], f = h->side[i];
+      if (e < 1 || e > K || f < 1 || f > 4) return set_err(nullptr, NEXD_ERR_INVALID, "halo: face element or side out of range");
+      const size_t k = size_t(4) * (e - 1) + (f - 1);
+      if (d->neighbor[k] != 0 || d->face[k] != NEXD_FACE_PARTITION)
+        return set_err(nullptr, NEXD_ERR_INVALID, "halo: face is not coded as shared (-3) in the descriptor");
+      if (seen[k]) return set_err(nullptr, NEXD_ERR_INVALID, "halo: face listed twice");
+      seen[k] = 1;
+      const int pi = h->peer_index[i];
+      if (pi < 1 || pi > h->nface[p] || used[pi - 1])
+        return set_err(nullptr, NEXD_ERR_INVALID, "halo: peer_index is not a permutation of the neighbour's faces");
+      used[pi - 1] = 1;
+      unsigned long long nodes = 0;
+      for (int j = 0; j < NpF; ++j) {
+        const int m = h->peer_node[i * NpF + j];
+        if (m < 1 || m > NpF || (nodes >> (m - 1) & 1ull))
+          return set_err(nullptr, NEXD_ERR_INVALID, "halo: peer_node is not a permutation of the face nodes");
+        nodes |= 1ull << (m - 1);
+      }
+    }
+  }
+  for (size_t k = 0; k < seen.size(); ++k)
+    if (d->face[k] == NEXD_FACE_PARTITION && d->neighbor[k] == 0 && !seen[k])
+      return set_err(nullptr, NEXD_ERR_INVALID, "halo: a shared face (-3) is missing from the halo");
   return NEXD_OK;
 }
 
@@ -440,11 +515,16 @@ int configure_launch(nexd_ctx* c) {
   return NEXD_OK;
 }
 
-int nexd_create(const nexd_desc* d, nexd_ctx** out) {
+}  // extern "C"
+
+namespace {
+
+int create_impl(const nexd_desc* d, const nexd_halo_desc* h, nexd_ctx** out) {
   if (!out) return set_err(nullptr, NEXD_ERR_INVALID, "null output pointer");
   *out = nullptr;
-  int st = validate(d);
+  int st = validate(d, h != nullptr);
   if (st) return st;
+  if (h && (st = validate_halo(d, h))) return st;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -458,6 +538,20 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   };
   const int N = d->N, Np = d->Np, NpF = d->NpF, K = d->nelem, NF = 4 * NpF;
   c->N = N; c->Np = Np; c->NpF = NpF; c->K = K;
+  // halo slot of each shared face: its position in the halo lists
+  std::vector<int> halo_slot;
+  if (h) {
+    c->partition = h->partition;
+    c->npeer = h->npeer;
+    halo_slot.assign(size_t(4) * K, -1);
+    for (int p = 0; p < h->npeer; ++p) {
+      c->peer_part.push_back(h->peer[p]);
+      c->peer_nface.push_back(h->nface[p]);
+      c->peer_goff.push_back(c->nhalo);
+      for (int i = 0; i < h->nface[p]; ++i, ++c->nhalo)
+        halo_slot[size_t(4) * (h->elem[c->nhalo] - 1) + (h->side[c->nhalo] - 1)] = c->nhalo;
+    }
+  }
   c->att = d->attenuation != 0;
   c->pml = d->set_pml != 0;
   c->nMB = c->att ? d->nMB : 0;
@@ -495,12 +589,18 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     const int e = c->new2old[ni];
     for (int f = 0; f < 4; ++f) {
       const int nb = d->neighbor[4 * e + f];
-      if (nb == 0) {
+      const bool shared = nb == 0 && d->face[4 * e + f] == NEXD_FACE_PARTITION;
+      if (nb == 0 && !shared) {
         h_fcode[4 * ni + f] = d->face[4 * e + f];  // -1 free, -2 absorbing
         continue;
       }
+      // a shared face reads its halo slot in its own face-node order
       std::vector<unsigned char> row(NpF);
       for (int i = 0; i < NpF; ++i) {
+        if (shared) {
+          row[i] = (unsigned char)i;
+          continue;
+        }
         const long long gn = (long long)d->ibn[(size_t(e) * 4 + f) * NpF + i] - 1 - (long long)(nb - 1) * Np;
         if (gn < 0 || gn >= Np) return fail(set_err(c, NEXD_ERR_INVALID, "ibn does not point into the neighbour element"));
         row[i] = (unsigned char)gn;
@@ -514,7 +614,7 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
       } else {
         id = it->second;
       }
-      h_nbr[4 * ni + f] = c->old2new[nb - 1];
+      h_nbr[4 * ni + f] = shared ? K + halo_slot[4 * e + f] : c->old2new[nb - 1];
       h_fcode[4 * ni + f] = id;
     }
   }
@@ -639,7 +739,7 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   }
 
   // ---- device memory ----
-  const long long nodes = (long long)K * Np;
+  const long long nodes = (long long)(K + c->nhalo) * Np;
   c->ldq = (nodes + 63) / 64 * 64;
   c->ldt = c->ldq;
   c->lda = ((long long)c->Kpml * Np + 63) / 64 * 64;
@@ -676,6 +776,38 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
     if ((st = dalloc(c, &c->qbuf[i], size_t(nb) * 9 * c->ldq))) return fail(st);
     if ((st = fill(c, c->qbuf[i], size_t(nb) * 9 * c->ldq, float(d->init_value)))) return fail(st);
     c->init_value = float(d->init_value);
+  }
+  if (h) {
+    // this partition's shared face nodes in neighbour order: own node, and
+    // the node offset in the neighbour's halo (slot of the same face there,
+    // matching node)
+    std::vector<int> hs, hd, blocks;
+    for (int p = 0, i = 0; p < c->npeer; ++p) {
+      HaloPeer hp{};
+      hp.entry0 = int(hs.size());
+      hp.block0 = c->put_blocks;
+      for (int k = 0; k < c->peer_nface[p]; ++k, ++i) {
+        const int ni = c->old2new[h->elem[i] - 1], f = h->side[i] - 1;
+        for (int j = 0; j < NpF; ++j) {
+          hs.push_back(ni * Np + d->fmask[f * NpF + j] - 1);
+          hd.push_back((h->peer_index[i] - 1) * Np + h->peer_node[i * NpF + j] - 1);
+        }
+      }
+      hp.nentry = int(hs.size()) - hp.entry0;
+      const int nbk = (hp.nentry + kHaloThreads - 1) / kHaloThreads;
+      blocks.push_back(nbk);  // the neighbour sends the same number (same shared faces)
+      c->put_blocks += nbk;
+      c->peers_h.push_back(hp);
+    }
+    c->peer_linked.assign(size_t(c->npeer), 0);
+    if (c->npeer > 0) {
+      if ((st = upload(c, &c->halo_src, hs)) || (st = upload(c, &c->halo_dst, hd)) ||
+          (st = upload(c, &c->halo_blocks, blocks)) || (st = dalloc(c, &c->peers_dev, size_t(c->npeer))) ||
+          (st = dalloc(c, &c->halo_counters, size_t(c->npeer))) || (st = dalloc(c, &c->halo_expected, size_t(c->npeer))))
+        return fail(st);
+      CUDA_TRY(c, cudaMemset(c->halo_counters, 0, c->npeer * sizeof(unsigned long long)));
+      CUDA_TRY(c, cudaMemset(c->halo_expected, 0, c->npeer * sizeof(unsigned long long)));
+    }
   }
   if (c->timeint == 4) {
     if ((st = dalloc(c, &c->res, size_t(nb) * 9 * c->ldq))) return fail(st);
@@ -778,6 +910,20 @@ int nexd_create(const nexd_desc* d, nexd_ctx** out) {
   CUDA_TRY(c, cudaDeviceSynchronize());
   *out = c;
   return NEXD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nexd_create(const nexd_desc* d, nexd_ctx** out) { return create_impl(d, nullptr, out); }
+
+int nexd_create_partition(const nexd_desc* d, const nexd_halo_desc* h, nexd_ctx** out) {
+  if (!h) {
+    if (out) *out = nullptr;
+    return set_err(nullptr, NEXD_ERR_INVALID, "null halo descriptor");
+  }
+  return create_impl(d, h, out);
 }
 
 namespace {
@@ -961,139 +1107,183 @@ void lserk_stage_args(nexd_ctx* c, int s, StageArgs& a) {
   a.e_end = c->K;
 }
 
+// The receiver gather at the start of a step.
+void enqueue_step_head(nexd_ctx* c) {
+  if (c->nrec * c->nbatch == 0) return;
+  const int ev = ev_begin(c, NEXD_K_RECORD);
+  enqueue_record(c, c->stream);
+  ev_end(c, ev);
+}
+
+// Arguments of stage s of the current step; *in and *outb receive the
+// buffers the stage reads and writes.
+void plan_stage(nexd_ctx* c, int s, StageArgs& a, int* in_buf, int* out_buf) {
+  a.stage = s;
+  a.last_stage = (s == c->nstage - 1);
+  a.stage_first = (s == 0);
+  int in = c->cur, outb;
+  const float* qn = nullptr;
+  if (c->timeint == 4) {
+    a.ca = float(kRK4A[s]);
+    a.cb = float(kRK4B[s]);
+    outb = 1 - c->cur;
+  } else if (c->timeint == 1) {
+    a.ca = 0.f; a.cb = 1.f;
+    outb = 1 - c->cur;
+  } else if (c->timeint == 2) {
+    // stage 1: A -> B; stage 2: (A, B) -> A  (src/rungekuttaMod.f90:90-103)
+    if (s == 0) { a.ca = 0.f; a.cb = 1.f; in = c->cur; outb = 1 - c->cur; }
+    else { a.ca = 0.5f; a.cb = 0.5f; in = 1 - c->cur; outb = c->cur; qn = c->qbuf[c->cur]; }
+  } else {
+    // RK3: A -> B; (A,B) -> C; (A,C) -> A  (src/rungekuttaMod.f90:105-120)
+    const int A = c->cur, B = (c->cur + 1) % 3, C = (c->cur + 2) % 3;
+    if (s == 0) { a.ca = 0.f; a.cb = 1.f; in = A; outb = B; }
+    else if (s == 1) { a.ca = 0.75f; a.cb = 0.25f; in = B; outb = C; qn = c->qbuf[A]; }
+    else { a.ca = float(1.0 / 3.0); a.cb = float(2.0 / 3.0); in = C; outb = A; qn = c->qbuf[A]; }
+  }
+  a.q_in = c->qbuf[in];
+  a.q_out = c->qbuf[outb];
+  a.q_n = qn;
+  *in_buf = in;
+  *out_buf = outb;
+}
+
+// This partition's shared face traces of buffer `in` into its neighbours'
+// halo slots (the stage's input), one arrival per write block.
+void enqueue_halo_put(nexd_ctx* c, int in) {
+  if (c->npeer == 0) return;
+  HaloPutArgs h{};
+  h.q = c->qbuf[in];
+  h.ldq = c->ldq;
+  h.nbatch = c->nbatch;
+  h.which = in;
+  h.npeer = c->npeer;
+  h.peers = c->peers_dev;
+  h.src = c->halo_src;
+  h.dst = c->halo_dst;
+  const int ev = ev_begin(c, NEXD_K_HALO);
+  halo_put_kernel<<<c->put_blocks, kHaloThreads, 0, c->stream>>>(h);
+  ev_end(c, ev);
+  ++c->launches;
+}
+
+// The stage waits for every neighbour's writes of this stage.
+void enqueue_halo_wait(nexd_ctx* c) {
+  if (c->npeer == 0) return;
+  HaloWaitArgs w{};
+  w.counters = c->halo_counters;
+  w.expected = c->halo_expected;
+  w.blocks = c->halo_blocks;
+  w.npeer = c->npeer;
+  w.limit_ns = c->halo_limit_ns;
+  w.flag = c->flag;
+  const int ev = ev_begin(c, NEXD_K_HALO);
+  halo_wait_kernel<<<1, 64, 0, c->stream>>>(w);
+  ev_end(c, ev);
+  ++c->launches;
+}
+
+// One stage's element loop: the learned-boundary exterior states (when on),
+// then the NPML and the other elements.
+void enqueue_stage_kernels(nexd_ctx* c, StageArgs& a) {
+  if (c->mlp_on) {
+    // exterior states of the absorbing faces from this stage's input
+    GhostArgs ga{};
+    ga.nbf = c->nbf;
+    ga.nbatch = c->nbatch;
+    ga.NpF = c->NpF;
+    ga.Np = c->Np;
+    ga.ldq = c->ldq;
+    ga.q = a.q_in;
+    ga.bf_elem = c->bf_elem;
+    ga.bf_face = c->bf_face;
+    ga.geo = c->geo;
+    ga.pat = c->patterns;
+    ga.w = c->mlp_w;
+    ga.rho_max = c->mlp_rho;
+    ga.ghost = c->ghost;
+    const int ev = ev_begin(c, NEXD_K_BOUNDARY);
+    ghost_kernel<<<c->ghost_grid, kGhostThreads, c->ghost_smem, c->stream>>>(ga);
+    ev_end(c, ev);
+    ++c->launches;
+  }
+  if (c->Kpml > 0) {
+    const int ev = ev_begin(c, NEXD_K_STAGE_PML);
+    launch_class(c, a, true);
+    ev_end(c, ev);
+    ++c->launches;
+  }
+  if (c->K > c->Kpml) {
+    const int ev = ev_begin(c, NEXD_K_STAGE_MAIN);
+    launch_class(c, a, false);
+    ev_end(c, ev);
+    ++c->launches;
+  }
+}
+
+void end_stage(nexd_ctx* c, int outb) {
+  if (c->timeint == 4 || c->timeint == 1) c->cur = outb;
+}
+
+// End of a step: NPML energy and trigger, movie frame, step counter.
+void enqueue_step_tail(nexd_ctx* c) {
+  if (c->energy_on) {
+    // wavefield energy of step it and the STA/LTA rule (src/timeloopMod.f90:508-542)
+    EnergyArgs ea{};
+    ea.K = c->K;
+    ea.Np = c->Np;
+    ea.nbatch = c->nbatch;
+    ea.ldq = c->ldq;
+    ea.q = c->qbuf[c->cur];
+    ea.emat = c->emat;
+    ea.mass = c->mass;
+    ea.partials = c->partials;
+    ea.formula = c->trig_formula;
+    const int E = kEnergyThreads / c->Np;
+    const size_t smem = (size_t(c->Np) * c->Np + size_t(E) * 9 * c->Np) * sizeof(double);
+    const int ev = ev_begin(c, NEXD_K_ENERGY);
+    energy_kernel<<<dim3(c->energy_blocks, c->nbatch), kEnergyThreads, smem, c->stream>>>(ea);
+    TriggerArgs ta{};
+    ta.partials = c->partials;
+    ta.nparts = c->energy_blocks;
+    ta.energy = c->energy;
+    ta.nt = c->nt;
+    ta.it_dev = c->it_dev;
+    ta.armed = 1;
+    ta.timecrit = c->trig_timecrit;
+    ta.w1 = c->trig_w1;
+    ta.w2 = c->trig_w2;
+    ta.threshold = c->trig_threshold;
+    ta.pml_off = c->pml_off;
+    ta.pml_switch = c->pml_switch;
+    energy_finalize<<<c->nbatch, 256, 0, c->stream>>>(ta);
+    ev_end(c, ev);
+    c->launches += 2;
+  }
+  if (c->movie_frame > 0) {
+    const int E = 256 / c->Np;
+    movie_kernel<<<dim3((c->K + E - 1) / E, c->nbatch), 256, 0, c->stream>>>(
+        c->qbuf[c->cur], c->movie_u, c->ldq, c->K, c->Np, c->nbatch, float(c->dt), c->it_dev, c->movie_frame,
+        c->movie_max, c->movie_buf);
+    ++c->launches;
+  }
+  tick_kernel<<<1, 32, 0, c->stream>>>(c->it_dev);
+  ++c->launches;
+}
+
 void enqueue_body(nexd_ctx* c, int nsteps) {
   StageArgs a = base_args(c);
-  RecordArgs r{};
-  r.nrec = c->nrec;
-  r.nbatch = c->nbatch;
-  r.Np = c->Np;
-  r.nt = c->nt;
-  r.ldq = c->ldq;
-  r.recelem = c->recelem;
-  r.recslot = c->recslot_of_rec;
-  r.recInt = c->recInt;
-  r.abuf = c->abuf;
-  r.nslot = std::max(1, c->nslot);
-  r.u = c->u;
-  r.traces = c->traces;
-  r.dt = float(c->dt);
-  r.flag = c->flag;
-  r.it_dev = c->it_dev;
-  const int rec_warps = c->nrec * c->nbatch;
   for (int step = 0; step < nsteps; ++step) {
-    if (rec_warps > 0) {
-      r.q = c->qbuf[c->cur];
-      const int threads = 128;
-      const int blocks = (rec_warps * 32 + threads - 1) / threads;
-      const int ev = ev_begin(c, NEXD_K_RECORD);
-      record_kernel<<<blocks, threads, 0, c->stream>>>(r);
-      ev_end(c, ev);
-      ++c->launches;
-    }
+    enqueue_step_head(c);
     for (int s = 0; s < c->nstage; ++s) {
-      a.stage = s;
-      a.last_stage = (s == c->nstage - 1);
-      a.stage_first = (s == 0);
-      int in = c->cur, outb;
-      const float* qn = nullptr;
-      if (c->timeint == 4) {
-        a.ca = float(kRK4A[s]);
-        a.cb = float(kRK4B[s]);
-        outb = 1 - c->cur;
-      } else if (c->timeint == 1) {
-        a.ca = 0.f; a.cb = 1.f;
-        outb = 1 - c->cur;
-      } else if (c->timeint == 2) {
-        // stage 1: A -> B; stage 2: (A, B) -> A  (src/rungekuttaMod.f90:90-103)
-        if (s == 0) { a.ca = 0.f; a.cb = 1.f; in = c->cur; outb = 1 - c->cur; }
-        else { a.ca = 0.5f; a.cb = 0.5f; in = 1 - c->cur; outb = c->cur; qn = c->qbuf[c->cur]; }
-      } else {
-        // RK3: A -> B; (A,B) -> C; (A,C) -> A  (src/rungekuttaMod.f90:105-120)
-        const int A = c->cur, B = (c->cur + 1) % 3, C = (c->cur + 2) % 3;
-        if (s == 0) { a.ca = 0.f; a.cb = 1.f; in = A; outb = B; }
-        else if (s == 1) { a.ca = 0.75f; a.cb = 0.25f; in = B; outb = C; qn = c->qbuf[A]; }
-        else { a.ca = float(1.0 / 3.0); a.cb = float(2.0 / 3.0); in = C; outb = A; qn = c->qbuf[A]; }
-      }
-      a.q_in = c->qbuf[in];
-      a.q_out = c->qbuf[outb];
-      a.q_n = qn;
-      if (c->mlp_on) {
-        // exterior states of the absorbing faces from this stage's input
-        GhostArgs ga{};
-        ga.nbf = c->nbf;
-        ga.nbatch = c->nbatch;
-        ga.NpF = c->NpF;
-        ga.Np = c->Np;
-        ga.ldq = c->ldq;
-        ga.q = a.q_in;
-        ga.bf_elem = c->bf_elem;
-        ga.bf_face = c->bf_face;
-        ga.geo = c->geo;
-        ga.pat = c->patterns;
-        ga.w = c->mlp_w;
-        ga.rho_max = c->mlp_rho;
-        ga.ghost = c->ghost;
-        const int ev = ev_begin(c, NEXD_K_BOUNDARY);
-        ghost_kernel<<<c->ghost_grid, kGhostThreads, c->ghost_smem, c->stream>>>(ga);
-        ev_end(c, ev);
-        ++c->launches;
-      }
-      if (c->Kpml > 0) {
-        const int ev = ev_begin(c, NEXD_K_STAGE_PML);
-        launch_class(c, a, true);
-        ev_end(c, ev);
-        ++c->launches;
-      }
-      if (c->K > c->Kpml) {
-        const int ev = ev_begin(c, NEXD_K_STAGE_MAIN);
-        launch_class(c, a, false);
-        ev_end(c, ev);
-        ++c->launches;
-      }
-      if (c->timeint == 4 || c->timeint == 1) c->cur = outb;
+      int in, outb;
+      plan_stage(c, s, a, &in, &outb);
+      enqueue_halo_put(c, in);
+      enqueue_halo_wait(c);
+      enqueue_stage_kernels(c, a);
+      end_stage(c, outb);
     }
-    if (c->energy_on) {
-      // wavefield energy of step it and the STA/LTA rule (src/timeloopMod.f90:508-542)
-      EnergyArgs ea{};
-      ea.K = c->K;
-      ea.Np = c->Np;
-      ea.nbatch = c->nbatch;
-      ea.ldq = c->ldq;
-      ea.q = c->qbuf[c->cur];
-      ea.emat = c->emat;
-      ea.mass = c->mass;
-      ea.partials = c->partials;
-      ea.formula = c->trig_formula;
-      const int E = kEnergyThreads / c->Np;
-      const size_t smem = (size_t(c->Np) * c->Np + size_t(E) * 9 * c->Np) * sizeof(double);
-      const int ev = ev_begin(c, NEXD_K_ENERGY);
-      energy_kernel<<<dim3(c->energy_blocks, c->nbatch), kEnergyThreads, smem, c->stream>>>(ea);
-      TriggerArgs ta{};
-      ta.partials = c->partials;
-      ta.nparts = c->energy_blocks;
-      ta.energy = c->energy;
-      ta.nt = c->nt;
-      ta.it_dev = c->it_dev;
-      ta.armed = 1;
-      ta.timecrit = c->trig_timecrit;
-      ta.w1 = c->trig_w1;
-      ta.w2 = c->trig_w2;
-      ta.threshold = c->trig_threshold;
-      ta.pml_off = c->pml_off;
-      ta.pml_switch = c->pml_switch;
-      energy_finalize<<<c->nbatch, 256, 0, c->stream>>>(ta);
-      ev_end(c, ev);
-      c->launches += 2;
-    }
-    if (c->movie_frame > 0) {
-      const int E = 256 / c->Np;
-      movie_kernel<<<dim3((c->K + E - 1) / E, c->nbatch), 256, 0, c->stream>>>(
-          c->qbuf[c->cur], c->movie_u, c->ldq, c->K, c->Np, c->nbatch, float(c->dt), c->it_dev, c->movie_frame,
-          c->movie_max, c->movie_buf);
-      ++c->launches;
-    }
-    tick_kernel<<<1, 32, 0, c->stream>>>(c->it_dev);
-    ++c->launches;
+    enqueue_step_tail(c);
   }
 }
 
@@ -1170,6 +1360,14 @@ int enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
 }
 
 // Synchronises, collects profiling events and checks the non-finite flag.
+// A partition steps only when every neighbour is linked.
+int check_linked(nexd_ctx* c) {
+  for (int p = 0; p < c->npeer; ++p)
+    if (!c->peer_linked[p])
+      return set_err(c, NEXD_ERR_INVALID, "partition not linked to all neighbours (nexd_halo_connect)");
+  return NEXD_OK;
+}
+
 int finish(nexd_ctx* c) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
@@ -1177,6 +1375,7 @@ int finish(nexd_ctx* c) {
   CUDA_TRY(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (c->profiling) ev_collect(c);
+  if (flag & 4) return set_err(c, NEXD_ERR_TIMEOUT, "halo arrival wait ran out: a neighbour partition did not write its traces");
   if (flag & 2) return set_err(c, NEXD_ERR_CUDA, "tensor-core completion wait timed out in a stage kernel");
   if (flag) return set_err(c, NEXD_ERR_NONFINITE, "non-finite value in the wavefield at a receiver");
   return NEXD_OK;
@@ -1187,6 +1386,7 @@ int finish(nexd_ctx* c) {
 int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
   if (it_begin < 1 || it_end > c->nt || it_begin > it_end) return set_err(c, NEXD_ERR_INVALID, "step range out of 1..nt");
+  if (int st = check_linked(c)) return st;
   if (c->span_timing) {
     if (!c->span[0]) {
       CUDA_TRY(c, cudaEventCreate(&c->span[0]));
@@ -1207,6 +1407,7 @@ int nexd_run(nexd_ctx* c, int32_t it_begin, int32_t it_end) {
 int nexd_step_io(nexd_ctx* c, int32_t it, const float* stf_in, float* traces_out) {
   if (!c || !traces_out) return set_err(c, NEXD_ERR_INVALID, "null argument");
   if (it < 1 || it > c->nt) return set_err(c, NEXD_ERR_INVALID, "step out of 1..nt");
+  if (int st = check_linked(c)) return st;
   const size_t nin = size_t(c->nspt) * c->nsrc, nout = size_t(c->nrec) * 9 * c->nbatch;
   if (!c->pinned || c->pinned_floats < nin + nout) return set_err(c, NEXD_ERR_INVALID, "no pinned staging buffer");
   if (stf_in && nin > 0) {
@@ -1368,6 +1569,8 @@ int nexd_pml_trigger(nexd_ctx* c, int32_t avg_window1, int32_t avg_window2, doub
                      int32_t formula) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
   if (!c->pml) return set_err(c, NEXD_ERR_INVALID, "the STA/LTA trigger needs set_pml");
+  if (c->partition > 0)
+    return set_err(c, NEXD_ERR_UNSUPPORTED, "the STA/LTA trigger sums the energy of the whole mesh: not on a partition");
   if (avg_window1 < 1 || avg_window2 < 1 || !(f0 > 0.0) || !(sta_lta_trigger >= 0.0) || (formula != 0 && formula != 1))
     return set_err(c, NEXD_ERR_INVALID, "bad trigger parameters");
   c->trig_w1 = avg_window1;
@@ -2194,6 +2397,179 @@ int nexd_wavefield_energy_noalloc(const float* q, int64_t ldq, int32_t nelem, in
   return NEXD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Partition halo: export / connect / in-process run
+// ---------------------------------------------------------------------------
+
+int nexd_halo_export_peer(nexd_ctx* c, int32_t peer, nexd_halo_export* out) {
+  if (!c || !out) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  if (peer < 0 || peer >= c->npeer) return set_err(c, NEXD_ERR_INVALID, "neighbour index out of range");
+  std::memset(out, 0, sizeof(*out));
+  out->abi_version = NEXD_ABI_VERSION;
+  out->device = c->device;
+  out->pid = int64_t(getpid());
+  out->partition = c->partition;
+  out->nface = c->peer_nface[peer];
+  out->nbatch = c->nbatch;
+  out->nbuf = c->timeint == 3 ? 3 : 2;
+  out->ldq = c->ldq;
+  out->halo_base = (long long)(c->K + c->peer_goff[peer]) * c->Np;
+  out->counter_slot = peer;
+  for (int i = 0; i < out->nbuf; ++i) {
+    out->q[i] = uint64_t(reinterpret_cast<uintptr_t>(c->qbuf[i]));
+    cudaIpcMemHandle_t hnd;
+    if (cudaIpcGetMemHandle(&hnd, c->qbuf[i]) == cudaSuccess) std::memcpy(out->q_ipc[i], &hnd, 64);
+    else cudaGetLastError();  // no IPC here: the export still links partitions of this process
+  }
+  out->counters = uint64_t(reinterpret_cast<uintptr_t>(c->halo_counters));
+  cudaIpcMemHandle_t hnd;
+  if (cudaIpcGetMemHandle(&hnd, c->halo_counters) == cudaSuccess) std::memcpy(out->counters_ipc, &hnd, 64);
+  else cudaGetLastError();
+  return NEXD_OK;
+}
+
+int nexd_halo_connect(nexd_ctx* c, int32_t peer, const nexd_halo_export* in) {
+  if (!c || !in) return set_err(c, NEXD_ERR_INVALID, "null argument");
+  if (peer < 0 || peer >= c->npeer) return set_err(c, NEXD_ERR_INVALID, "neighbour index out of range");
+  if (in->abi_version != NEXD_ABI_VERSION) return set_err(c, NEXD_ERR_INVALID, "halo export: ABI version mismatch");
+  if (in->partition != c->peer_part[peer])
+    return set_err(c, NEXD_ERR_INVALID, "halo export comes from another partition than this neighbour");
+  if (in->nface != c->peer_nface[peer])
+    return set_err(c, NEXD_ERR_INVALID, "halo export: the neighbour shares a different number of faces");
+  if (in->nbatch != c->nbatch || in->nbuf != (c->timeint == 3 ? 3 : 2))
+    return set_err(c, NEXD_ERR_INVALID, "halo export: wavefield count or integrator differs from this partition");
+  if (in->counter_slot < 0 || in->counter_slot >= kHaloMaxPeers || in->ldq <= 0 || in->halo_base < 0 ||
+      in->halo_base + (long long)in->nface * c->Np > in->ldq)
+    return set_err(c, NEXD_ERR_INVALID, "halo export: inconsistent layout");
+  HaloPeer& hp = c->peers_h[peer];
+  hp.ldq = in->ldq;
+  hp.base = in->halo_base;
+  if (in->pid == int64_t(getpid())) {
+    // a partition of this process: its device addresses as they are
+    for (int i = 0; i < 3; ++i) hp.q[i] = i < in->nbuf ? reinterpret_cast<float*>(uintptr_t(in->q[i])) : nullptr;
+    hp.counter = reinterpret_cast<unsigned long long*>(uintptr_t(in->counters)) + in->counter_slot;
+    if (in->device != c->device) {
+      const cudaError_t e = cudaDeviceEnablePeerAccess(in->device, 0);
+      if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled)
+        return set_err(c, NEXD_ERR_CUDA, std::string("peer access to the neighbour's GPU: ") + cudaGetErrorString(e));
+      cudaGetLastError();
+    }
+  } else {
+    // another process: open its buffers through CUDA IPC (peer access enabled on first use)
+    auto open = [&](const unsigned char* bytes, void** p) -> int {
+      cudaIpcMemHandle_t hnd;
+      std::memcpy(&hnd, bytes, 64);
+      const cudaError_t e = cudaIpcOpenMemHandle(p, hnd, cudaIpcMemLazyEnablePeerAccess);
+      if (e != cudaSuccess) return set_err(c, NEXD_ERR_CUDA, std::string("cudaIpcOpenMemHandle: ") + cudaGetErrorString(e));
+      c->ipc_opened.push_back(*p);
+      return NEXD_OK;
+    };
+    for (int i = 0; i < 3; ++i) {
+      hp.q[i] = nullptr;
+      if (i >= in->nbuf) continue;
+      void* p = nullptr;
+      if (int st = open(in->q_ipc[i], &p)) return st;
+      hp.q[i] = static_cast<float*>(p);
+    }
+    void* p = nullptr;
+    if (int st = open(in->counters_ipc, &p)) return st;
+    hp.counter = static_cast<unsigned long long*>(p) + in->counter_slot;
+  }
+  CUDA_TRY(c, cudaMemcpy(c->peers_dev + peer, &hp, sizeof(HaloPeer), cudaMemcpyHostToDevice));
+  const unsigned long long zero = 0;
+  CUDA_TRY(c, cudaMemcpy(c->halo_counters + peer, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->halo_expected + peer, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+  c->peer_linked[peer] = 1;
+  drop_graphs(c);  // captured graphs hold the neighbour table as it was
+  return NEXD_OK;
+}
+
+int nexd_halo_set_timeout(nexd_ctx* c, double seconds) {
+  if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
+  if (!(seconds > 0.0) || seconds > 60.0) return set_err(c, NEXD_ERR_INVALID, "halo wait limit out of (0, 60] s");
+  c->halo_limit_ns = (unsigned long long)(seconds * 1e9);
+  drop_graphs(c);  // captured graphs hold the old limit
+  return NEXD_OK;
+}
+
+int nexd_halo_bytes(const nexd_ctx* c, int64_t* bytes) {
+  if (!c || !bytes) return set_err(nullptr, NEXD_ERR_INVALID, "null argument");
+  long long n = 0;
+  for (int p = 0; p < c->npeer; ++p) n += (long long)c->peer_nface[p] * c->NpF;
+  *bytes = n * 9 * c->nbatch * int64_t(sizeof(float));
+  return NEXD_OK;
+}
+
+int nexd_halo_run(nexd_ctx* const* parts, int32_t n, int32_t it_begin, int32_t it_end) {
+  if (!parts || n < 1) return set_err(nullptr, NEXD_ERR_INVALID, "no partitions");
+  for (int i = 0; i < n; ++i) {
+    nexd_ctx* c = parts[i];
+    if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null partition");
+    for (int j = 0; j < i; ++j)
+      if (parts[j] == c) return set_err(c, NEXD_ERR_INVALID, "partition listed twice");
+    if (it_begin < 1 || it_end > c->nt || it_begin > it_end) return set_err(c, NEXD_ERR_INVALID, "step range out of 1..nt");
+    if (int st = check_linked(c)) return st;
+    if (c->device != parts[0]->device || c->timeint != parts[0]->timeint || c->cur != parts[0]->cur)
+      return set_err(c, NEXD_ERR_INVALID, "partitions must share the GPU, the integrator and the step");
+  }
+  // every neighbour written to must be one of the partitions run here
+  for (int i = 0; i < n; ++i)
+    for (int p = 0; p < parts[i]->npeer; ++p) {
+      bool found = false;
+      for (int j = 0; j < n; ++j) found = found || parts[j]->partition == parts[i]->peer_part[p];
+      if (!found) return set_err(parts[i], NEXD_ERR_INVALID, "a neighbour partition is not in this run");
+    }
+  // one stream for all: each stage's writes come before every wait on them
+  cudaStream_t s = parts[0]->stream;
+  std::vector<cudaStream_t> own(n);
+  for (int i = 0; i < n; ++i) {
+    own[i] = parts[i]->stream;
+    CUDA_TRY(parts[i], cudaStreamSynchronize(own[i]));
+    parts[i]->stream = s;
+    parts[i]->movie_last_it = std::max(parts[i]->movie_last_it, it_end);
+    set_step_kernel<<<1, 32, 0, s>>>(parts[i]->it_dev, it_begin);
+  }
+  // run span on the shared stream, booked to the first partition
+  nexd_ctx* p0 = parts[0];
+  if (p0->span_timing) {
+    if (!p0->span[0]) {
+      CUDA_TRY(p0, cudaEventCreate(&p0->span[0]));
+      CUDA_TRY(p0, cudaEventCreate(&p0->span[1]));
+    }
+    CUDA_TRY(p0, cudaEventRecord(p0->span[0], s));
+  }
+  std::vector<StageArgs> a(n);
+  for (int i = 0; i < n; ++i) a[i] = base_args(parts[i]);
+  std::vector<int> in(n), outb(n);
+  for (int it = it_begin; it <= it_end; ++it) {
+    for (int i = 0; i < n; ++i) enqueue_step_head(parts[i]);
+    for (int st = 0; st < parts[0]->nstage; ++st) {
+      for (int i = 0; i < n; ++i) {
+        plan_stage(parts[i], st, a[i], &in[i], &outb[i]);
+        enqueue_halo_put(parts[i], in[i]);
+      }
+      for (int i = 0; i < n; ++i) {
+        enqueue_halo_wait(parts[i]);
+        enqueue_stage_kernels(parts[i], a[i]);
+        end_stage(parts[i], outb[i]);
+      }
+    }
+    for (int i = 0; i < n; ++i) enqueue_step_tail(parts[i]);
+  }
+  if (p0->span_timing) CUDA_TRY(p0, cudaEventRecord(p0->span[1], s));
+  int status = NEXD_OK;
+  for (int i = 0; i < n; ++i) {
+    const int st = finish(parts[i]);
+    if (st && status == NEXD_OK) status = st;
+  }
+  if (p0->span_timing && status == NEXD_OK) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p0->span[0], p0->span[1]) == cudaSuccess) p0->prof.span_ms += ms;
+  }
+  for (int i = 0; i < n; ++i) parts[i]->stream = own[i];
+  return status;
+}
+
 int nexd_profile_enable(nexd_ctx* c, int32_t on) {
   if (!c) return set_err(nullptr, NEXD_ERR_INVALID, "null context");
   if (on < 0 || on > 2) return set_err(c, NEXD_ERR_INVALID, "timing mode must be 0, 1 or 2");
@@ -2315,6 +2691,7 @@ int nexd_destroy(nexd_ctx* c) {
   if (!c) return NEXD_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
+  for (void* p : c->ipc_opened) cudaIpcCloseMemHandle(p);
   for (void* p : c->allocations) cudaFree(p);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   for (cudaEvent_t e : c->span)

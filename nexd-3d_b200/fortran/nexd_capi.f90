@@ -21,6 +21,7 @@ module nexd_capi
 
   integer(c_int32_t), parameter :: NEXD_ABI_VERSION = 1
   integer(c_int32_t), parameter :: NEXD_CONTRACT_FP32 = 0, NEXD_CONTRACT_BF16X3 = 1, NEXD_CONTRACT_AUTO = 2
+  integer(c_int32_t), parameter :: NEXD_FACE_PARTITION = -3
 
   type, bind(C) :: nexd_desc
      integer(c_int32_t) :: abi_version, N, Np, NpF, nelem, nMB, attenuation, set_pml, timeint, nt
@@ -40,11 +41,50 @@ module nexd_capi
      type(c_ptr) :: srcbatch
   end type nexd_desc
 
+  ! a partition's interface (nexd_create_partition): the mesher's
+  ! mpi_neighbor / mpi_ninterface / mpi_connection / mpi_ibool / mpi_ibt
+  type, bind(C) :: nexd_halo_desc
+     integer(c_int32_t) :: partition, npeer
+     type(c_ptr) :: peer, nface, elem, side, peer_index, peer_node
+  end type nexd_halo_desc
+
+  ! what a neighbour needs to write into this partition, sent as bytes
+  type, bind(C) :: nexd_halo_export
+     integer(c_int32_t) :: abi_version, device
+     integer(c_int64_t) :: pid
+     integer(c_int32_t) :: partition, nface, nbatch, nbuf
+     integer(c_int64_t) :: ldq, halo_base
+     integer(c_int32_t) :: counter_slot, reserved
+     integer(c_int64_t) :: q(3), counters
+     integer(c_int8_t) :: q_ipc(64,3), counters_ipc(64)
+  end type nexd_halo_export
+
   interface
      integer(c_int) function nexd_create(d, ctx) bind(C, name="nexd_create")
        import :: nexd_desc, c_ptr, c_int
        type(nexd_desc), intent(in) :: d
        type(c_ptr), intent(out) :: ctx
+     end function
+
+     integer(c_int) function nexd_create_partition(d, h, ctx) bind(C, name="nexd_create_partition")
+       import :: nexd_desc, nexd_halo_desc, c_ptr, c_int
+       type(nexd_desc), intent(in) :: d
+       type(nexd_halo_desc), intent(in) :: h
+       type(c_ptr), intent(out) :: ctx
+     end function
+
+     integer(c_int) function nexd_halo_export_peer(ctx, peer, ex) bind(C, name="nexd_halo_export_peer")
+       import :: nexd_halo_export, c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: peer
+       type(nexd_halo_export), intent(out) :: ex
+     end function
+
+     integer(c_int) function nexd_halo_connect(ctx, peer, ex) bind(C, name="nexd_halo_connect")
+       import :: nexd_halo_export, c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: peer
+       type(nexd_halo_export), intent(in) :: ex
      end function
 
      integer(c_int) function nexd_run(ctx, it_begin, it_end) bind(C, name="nexd_run")

@@ -17,8 +17,16 @@
 ! the reference's source term uses them (one sample per step, its moment
 ! sources already differentiated by prepareSources).
 !
-! Differences, each stated where it applies: one mesh partition per GPU
-! (par%nproc > 1 stops, the mesher must be run with nproc = 1); the NPML
+! A partitioned mesh (par%nproc > 1, one rank per GPU) keeps the mesher's
+! interface arrays: the faces the reference marks neighbor = -1 become
+! NEXD_FACE_PARTITION faces, mpi_neighbor / mpi_ninterface / mpi_connection /
+! mpi_ibool / mpi_ibt fill the halo descriptor of nexd_create_partition, and
+! every rank trades one halo export per neighbour with MPI_Sendrecv before the
+! loop; the per-stage exchange of SendRecVar (src/mpiMod.f90:310-351) then
+! runs inside the library (peer stores over NVLink).
+!
+! Differences, each stated where it applies: the NPML energy trigger sums the
+! energy of one partition, so it is armed only when par%nproc = 1; the NPML
 ! auxiliary update uses each element's own flux (the reference applies the
 ! last element's flux to every PML element, src/rungekuttaMod.f90:52-63);
 ! movie frames are not written (nexd_movie gives the element means that
@@ -43,6 +51,8 @@ module timeloopMod
     use pmlMod
     use typeMod
     use allocateMod
+    use mpiMod
+    use mpiincludeMod
     use nexd_capi
     implicit none
 
@@ -80,17 +90,19 @@ contains
         real(c_float), dimension(:,:,:,:), allocatable, target :: traces
         real(c_double), dimension(:), allocatable, target :: energy
         integer(c_int32_t), dimension(1), target :: pml_switch
+        ! partition interface (par%nproc > 1)
+        type(nexd_halo_desc), target :: h
+        type(nexd_halo_export), target :: ex_out, ex_in
+        integer(c_int32_t), dimension(:), allocatable, target :: hpeer, hnface, helem, hside, hpidx
+        integer(c_int32_t), dimension(:,:), allocatable, target :: hpnode
+        integer :: npeer, ntot, ierr, nbytes
+        integer, dimension(MPI_STATUS_SIZE) :: mpistat
         type(c_ptr) :: ctx
         integer(c_int) :: st
         integer :: ie, is, i, j, r, c, it, K, nsrc, nrec
         character(len=3), parameter :: xyz = 'xyz', kinds = 'uva'  ! seismo.{x,y,z}.%07d.sd{u,v,a}
         integer, dimension(Np) :: iv
         character(len=256) :: filename, path      ! plotPoints2d takes a character(len=80) name
-
-        if (par%nproc > 1) then
-            write(*,*) 'timeloop3D: this solver runs one mesh partition per GPU; run the mesher with nproc = 1'
-            stop
-        end if
 
 ! load database, sources and receivers (src/timeloopMod.f90:137-159)
         call readMesh(myrank, mesh)
@@ -200,6 +212,47 @@ contains
         nbr4 = mesh%neighbor
         face4 = mesh%face
         ibn4 = mesh%ibn
+        if (par%nproc > 1) then
+            ! faces shared with another partition (neighbor = -1, src/meshMod.f90:776-784)
+            do ie = 1, K
+                do is = 1, 4
+                    if (mesh%neighbor(is,ie) == -1) then
+                        nbr4(is,ie) = 0
+                        face4(is,ie) = NEXD_FACE_PARTITION
+                    end if
+                end do
+            end do
+            ! the interface of this partition (src/meshMod.f90:1006-1110)
+            npeer = mesh%mpi_nn
+            allocate(hpeer(max(npeer,1)), hnface(max(npeer,1)))
+            if (npeer > 0) then
+                hpeer(1:npeer) = mesh%mpi_neighbor(1:npeer)
+                hnface(1:npeer) = mesh%mpi_ninterface(1:npeer)
+            end if
+            ntot = 0
+            if (npeer > 0) ntot = sum(hnface(1:npeer))
+            allocate(helem(max(ntot,1)), hside(max(ntot,1)), hpidx(max(ntot,1)), hpnode(NpF,max(ntot,1)))
+            c = 0
+            do i = 1, npeer
+                do j = 1, hnface(i)
+                    c = c + 1
+                    ie = mesh%mpi_connection(i,j,1)
+                    is = mesh%mpi_connection(i,j,2)
+                    helem(c) = ie
+                    hside(c) = is
+                    hpidx(c) = mesh%mpi_ibool(is,ie)       ! index of the face in the neighbour's list
+                    hpnode(:,c) = mesh%mpi_ibt(:,is,ie)    ! node matching, in the neighbour's face order
+                end do
+            end do
+            h%partition = myrank + 1
+            h%npeer = npeer
+            h%peer = c_loc(hpeer)
+            h%nface = c_loc(hnface)
+            h%elem = c_loc(helem)
+            h%side = c_loc(hside)
+            h%peer_index = c_loc(hpidx)
+            h%peer_node = c_loc(hpnode)
+        end if
 
 ! the descriptor (include/nexd.h: nexd_desc)
         d%abi_version = NEXD_ABI_VERSION
@@ -267,9 +320,25 @@ contains
         d%srcbatch = c_null_ptr
 
 ! the time loop (src/timeloopMod.f90:357-589) on the GPU
-        st = nexd_create(d, ctx)
-        call nexd_check(c_null_ptr, st)
-        if (par%set_pml) then
+        if (par%nproc > 1) then
+            st = nexd_create_partition(d, h, ctx)
+            call nexd_check(c_null_ptr, st)
+            ! one halo export per neighbour, traded with that neighbour's rank
+            nbytes = int(c_sizeof(ex_out))
+            do i = 1, npeer
+                st = nexd_halo_export_peer(ctx, int(i-1, c_int32_t), ex_out)
+                call nexd_check(ctx, st)
+                call MPI_SENDRECV(ex_out, nbytes, MPI_BYTE, hpeer(i)-1, 77, ex_in, nbytes, MPI_BYTE, hpeer(i)-1, 77, &
+                                  MPI_COMM_WORLD, mpistat, ierr)
+                st = nexd_halo_connect(ctx, int(i-1, c_int32_t), ex_in)
+                call nexd_check(ctx, st)
+            end do
+            call sync_mpi()        ! every partition linked before any writes into a neighbour
+        else
+            st = nexd_create(d, ctx)
+            call nexd_check(c_null_ptr, st)
+        end if
+        if (par%set_pml .and. par%nproc == 1) then
             ! the reference's STA/LTA trigger with its own energy expression (formula 0)
             st = nexd_pml_trigger(ctx, int(par%avg_window1, c_int32_t), int(par%avg_window2, c_int32_t), &
                                   real(par%sta_lta_trigger, c_double), real(f0, c_double), 0_c_int32_t)
@@ -286,7 +355,7 @@ contains
             st = nexd_get_traces(ctx, traces)
             call nexd_check(ctx, st)
         end if
-        if (par%set_pml) then
+        if (par%set_pml .and. par%nproc == 1) then
             st = nexd_get_energy(ctx, energy, pml_switch)
             call nexd_check(ctx, st)
             if (pml_switch(1) > 0) write(*,*) 'PML was switched off at time step ', pml_switch(1)
@@ -319,6 +388,7 @@ contains
         deallocate(Dr8, Ds8, Dt8, lift8, invmass8, fmask4, metric8, jac8, fscale8, nn8, ss8, tt8)
         deallocate(rho8, vpu8, vsu8, lam8, mu8, ylam8, ymu8, wl8, nbr4, face4, ibn4)
         if (allocated(prof8)) deallocate(prof8)
+        if (allocated(hpeer)) deallocate(hpeer, hnface, helem, hside, hpidx, hpnode)
         if (mesh%has_src) then
             deallocate(srcInt, t0, plotstf, Ms, srcelem4, srctype4, srcInt8, force8, srcM8, stf8)
             call deallocSrcVar(src)

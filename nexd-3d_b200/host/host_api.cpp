@@ -5,6 +5,11 @@
 
 #include "../../include/nexd_host.h"
 #include "mesh_db.hpp"
+#include "partition.hpp"
+
+struct nexd_partition {
+  std::vector<nexd::PartData> parts;
+};
 
 struct nexd_mesh {
   nexd::MeshDB db;
@@ -123,6 +128,52 @@ int nexd_mesh_write_seismograms(const nexd_mesh* mesh, const char* outdir, const
     return fail(e.what());
   }
 }
+
+int nexd_partition_create(const nexd_desc* desc, int32_t nparts, const int32_t* part, const double* centroid,
+                          nexd_partition** out) {
+  if (!desc || !out) return fail("nexd_partition_create: null argument");
+  *out = nullptr;
+  if (desc->abi_version != NEXD_ABI_VERSION) return fail("nexd_partition_create: ABI version mismatch");
+  try {
+    std::vector<int32_t> p;
+    if (part) p.assign(part, part + desc->nelem);
+    else p = nexd::bisect_partition(centroid, desc->nelem, nparts);
+    auto* ps = new nexd_partition;
+    try {
+      nexd::split_descriptor(*desc, p, nparts, ps->parts);
+    } catch (...) {
+      delete ps;
+      throw;
+    }
+    *out = ps;
+    return NEXD_OK;
+  } catch (const std::exception& e) {
+    return fail(e.what());
+  }
+}
+
+int nexd_partition_get(const nexd_partition* ps, int32_t index, nexd_part_view* out) {
+  if (!ps || !out) return fail("nexd_partition_get: null argument");
+  if (index < 0 || index >= int32_t(ps->parts.size())) return fail("nexd_partition_get: index out of range");
+  const nexd::PartData& d = ps->parts[index];
+  out->desc = &d.desc;
+  out->halo = &d.halo;
+  out->nelem = int32_t(d.elem_global.size());
+  out->elem_global = d.elem_global.data();
+  out->nsrc = int32_t(d.src_global.size());
+  out->src_global = d.src_global.data();
+  out->nrec = int32_t(d.rec_global.size());
+  out->rec_global = d.rec_global.data();
+  return NEXD_OK;
+}
+
+int nexd_partition_count(const nexd_partition* ps, int32_t* n) {
+  if (!ps || !n) return fail("nexd_partition_count: null argument");
+  *n = int32_t(ps->parts.size());
+  return NEXD_OK;
+}
+
+void nexd_partition_free(nexd_partition* ps) { delete ps; }
 
 int nexd_mesh_last_error(char* buf, size_t len) {
   if (!buf || len == 0) return NEXD_ERR_INVALID;

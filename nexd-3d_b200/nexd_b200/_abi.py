@@ -16,6 +16,8 @@ NEXD_ERR_NOMEM = 3
 NEXD_ERR_UNSUPPORTED = 4
 NEXD_ERR_NONFINITE = 5
 NEXD_ERR_NODEVICE = 6
+NEXD_ERR_TIMEOUT = 7
+NEXD_FACE_PARTITION = -3
 NEXD_NCOMP = 9
 NEXD_ABI_VERSION = 1
 
@@ -42,6 +44,25 @@ class NexdDesc(C.Structure):
     ]
 
 
+class NexdHaloDesc(C.Structure):
+    _fields_ = [("partition", C.c_int32), ("npeer", C.c_int32), ("peer", _pi), ("nface", _pi), ("elem", _pi),
+                ("side", _pi), ("peer_index", _pi), ("peer_node", _pi)]
+
+
+class NexdHaloExport(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("device", C.c_int32), ("pid", C.c_int64), ("partition", C.c_int32),
+                ("nface", C.c_int32), ("nbatch", C.c_int32), ("nbuf", C.c_int32), ("ldq", C.c_int64),
+                ("halo_base", C.c_int64), ("counter_slot", C.c_int32), ("reserved", C.c_int32),
+                ("q", C.c_uint64 * 3), ("counters", C.c_uint64), ("q_ipc", (C.c_ubyte * 64) * 3),
+                ("counters_ipc", C.c_ubyte * 64)]
+
+
+class NexdPartView(C.Structure):
+    _fields_ = [("desc", C.POINTER(NexdDesc)), ("halo", C.POINTER(NexdHaloDesc)), ("nelem", C.c_int32),
+                ("elem_global", _pi), ("nsrc", C.c_int32), ("src_global", _pi), ("nrec", C.c_int32),
+                ("rec_global", _pi)]
+
+
 class NexdBuildOpts(C.Structure):
     _fields_ = [
         ("N", C.c_int32), ("timeint", C.c_int32), ("cfl", C.c_double), ("nt", C.c_int32), ("t0", C.c_double),
@@ -60,8 +81,10 @@ class NexdMeshInfo(C.Structure):
 
 # Entry points declared in include/*.h, per library (checked by the CPU tests).
 HOST_SYMBOLS = ["nexd_mesh_build", "nexd_mesh_desc", "nexd_mesh_get_info", "nexd_mesh_write_seismograms",
-                "nexd_mesh_last_error", "nexd_mesh_free", "nexd_mesh_write_database", "nexd_mesh_load_database"]
-GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
+                "nexd_mesh_last_error", "nexd_mesh_free", "nexd_mesh_write_database", "nexd_mesh_load_database",
+                "nexd_partition_create", "nexd_partition_get", "nexd_partition_count", "nexd_partition_free"]
+GPU_SYMBOLS = ["nexd_create", "nexd_create_partition", "nexd_halo_export_peer", "nexd_halo_connect",
+               "nexd_halo_run", "nexd_halo_bytes", "nexd_halo_set_timeout", "nexd_run", "nexd_get_traces", "nexd_get_field", "nexd_set_field",
                "nexd_get_state", "nexd_set_state", "nexd_step_io", "nexd_pml_trigger", "nexd_get_energy",
                "nexd_set_contraction", "nexd_get_contraction", "nexd_set_contraction_kinds", "nexd_boundary_faces", "nexd_set_boundary_mlp",
                "nexd_get_ghost", "nexd_get_face_traces", "nexd_mlp_param_count", "nexd_mlp_workspace_floats",
@@ -70,7 +93,8 @@ GPU_SYMBOLS = ["nexd_create", "nexd_run", "nexd_get_traces", "nexd_get_field", "
                "nexd_group_get_mode", "nexd_movie", "nexd_get_movie",
                "nexd_wavefield_energy_noalloc", "nexd_profile_enable", "nexd_profile_get",
                "nexd_last_error", "nexd_launch_count", "nexd_destroy"]
-NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_ENERGY, NEXD_K_BOUNDARY, NEXD_K_COUNT = 0, 1, 2, 3, 4, 5
+NEXD_K_RECORD, NEXD_K_STAGE_PML, NEXD_K_STAGE_MAIN, NEXD_K_ENERGY, NEXD_K_BOUNDARY, NEXD_K_HALO, NEXD_K_COUNT = \
+    0, 1, 2, 3, 4, 5, 6
 
 
 class NexdProfile(C.Structure):
@@ -112,6 +136,14 @@ def host_lib():
         lib.nexd_mesh_last_error.restype = C.c_int
         lib.nexd_mesh_free.argtypes = [C.c_void_p]
         lib.nexd_mesh_free.restype = None
+        lib.nexd_partition_create.argtypes = [C.POINTER(NexdDesc), C.c_int32, _pi, _pd, C.POINTER(C.c_void_p)]
+        lib.nexd_partition_create.restype = C.c_int
+        lib.nexd_partition_get.argtypes = [C.c_void_p, C.c_int32, C.POINTER(NexdPartView)]
+        lib.nexd_partition_get.restype = C.c_int
+        lib.nexd_partition_count.argtypes = [C.c_void_p, _pi]
+        lib.nexd_partition_count.restype = C.c_int
+        lib.nexd_partition_free.argtypes = [C.c_void_p]
+        lib.nexd_partition_free.restype = None
         _host = lib
     return _host
 
@@ -122,6 +154,12 @@ def gpu_lib():
         lib = _load("libnexd.so")
         vp = C.c_void_p
         lib.nexd_create.argtypes = [C.POINTER(NexdDesc), C.POINTER(vp)]
+        lib.nexd_create_partition.argtypes = [C.POINTER(NexdDesc), C.POINTER(NexdHaloDesc), C.POINTER(vp)]
+        lib.nexd_halo_export_peer.argtypes = [vp, C.c_int32, C.POINTER(NexdHaloExport)]
+        lib.nexd_halo_connect.argtypes = [vp, C.c_int32, C.POINTER(NexdHaloExport)]
+        lib.nexd_halo_run.argtypes = [C.POINTER(vp), C.c_int32, C.c_int32, C.c_int32]
+        lib.nexd_halo_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
+        lib.nexd_halo_set_timeout.argtypes = [vp, C.c_double]
         lib.nexd_run.argtypes = [vp, C.c_int32, C.c_int32]
         lib.nexd_get_traces.argtypes = [vp, C.POINTER(C.c_float)]
         lib.nexd_get_field.argtypes = [vp, C.c_int32, C.POINTER(C.c_float)]

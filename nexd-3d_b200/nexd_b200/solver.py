@@ -19,12 +19,16 @@ def _gpu_error(ctx, status):
 
 
 class Solver:
-    """One device context: nexd_create on a descriptor, then run/traces."""
+    """One device context: nexd_create on a descriptor (nexd_create_partition
+    when a halo descriptor is given), then run/traces."""
 
-    def __init__(self, desc_ptr):
+    def __init__(self, desc_ptr, halo_ptr=None):
         lib = _abi.gpu_lib()
         ctx = C.c_void_p()
-        st = lib.nexd_create(desc_ptr, C.byref(ctx))
+        if halo_ptr is None:
+            st = lib.nexd_create(desc_ptr, C.byref(ctx))
+        else:
+            st = lib.nexd_create_partition(desc_ptr, halo_ptr, C.byref(ctx))
         if st != 0:
             raise _gpu_error(None, st)
         self._ctx = ctx
@@ -84,7 +88,7 @@ class Solver:
             return None
         p = _abi.NexdProfile()
         lib.nexd_profile_get(self._ctx, C.byref(p))
-        names = ("record", "stage_pml", "stage_main", "energy", "boundary")
+        names = ("record", "stage_pml", "stage_main", "energy", "boundary", "halo")
         out = {n: dict(launches=p.launches[i], ms=p.ms[i], elements=p.elements[i]) for i, n in enumerate(names)}
         out["span_ms"] = p.span_ms
         return out
