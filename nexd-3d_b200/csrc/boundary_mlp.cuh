@@ -1,6 +1,8 @@
 // Learned absorbing boundary: a per-face MLP that predicts the exterior
-// (ghost) state of an absorbing face from the interior face trace, and the
-// FP32 training kernels (forward, backward, Adam) for it.
+// (ghost) state of an absorbing face from the interior face trace -- its
+// features and arguments here, its tensor-core kernel in boundary_tc.cuh --
+// and the elementwise training kernels (the training GEMMs are in
+// mlp_tc.cuh).
 //
 // The reference's absorbing faces take the exterior state as zero, so the
 // upwind flux only removes the incoming characteristics
@@ -96,199 +98,10 @@ struct GhostArgs {
   float* ghost;              // [b][nbf][9][NpF]
 };
 
-constexpr int kGhostFaces = 16;  // faces per block pass
-constexpr int kGhostThreads = 256;
-
-// Shared memory: bf16 parameters + activation tiles [k][face] in FP32
-// (features, two hidden layers, prediction) + the RMS scales.
-__host__ __device__ constexpr size_t ghost_smem_bytes(int nin) {
-  return size_t(mlp_param_count(nin, kMlpHidden)) * 2 + 16 +
-         size_t(2 * nin + 2 * kMlpHidden + 1) * kGhostFaces * 4 + 16;
-}
-
-// Persistent: each block stages the bf16 parameters once, then loops over
-// groups of kGhostFaces (batch member, face) pairs.  Layers: thread j of each
-// half-block computes neuron j for 8 faces (FP32 accumulation).
-__global__ void __launch_bounds__(kGhostThreads) ghost_kernel(const GhostArgs a) {
-  extern __shared__ __align__(16) unsigned char gsm[];
-  const int nin = 9 * a.NpF, H = kMlpHidden;
-  const long long np_ = mlp_param_count(nin, H);
-  __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(gsm);
-  float* sx = reinterpret_cast<float*>(gsm + ((np_ * 2 + 15) / 16) * 16);  // [nin][F]
-  float* sh1 = sx + nin * kGhostFaces;                                      // [H][F]
-  float* sh2 = sh1 + H * kGhostFaces;                                       // [H][F]
-  float* sy = sh2 + H * kGhostFaces;                                        // [nin][F] prediction
-  float* sr = sy + nin * kGhostFaces;                                       // [F] RMS scale
-  const int tid = threadIdx.x;
-  {
-    const uint4* src = reinterpret_cast<const uint4*>(a.w);
-    uint4* dst = reinterpret_cast<uint4*>(sw);
-    const long long n16 = np_ * 2 / 16;
-    for (long long i = tid; i < n16; i += blockDim.x) dst[i] = src[i];
-    for (long long i = n16 * 8 + tid; i < np_; i += blockDim.x) sw[i] = a.w[i];
-  }
-  const __nv_bfloat16* W1 = sw;
-  const __nv_bfloat16* b1 = W1 + (long long)H * nin;
-  const __nv_bfloat16* W2 = b1 + H;
-  const __nv_bfloat16* b2 = W2 + (long long)H * H;
-  const __nv_bfloat16* W3 = b2 + H;
-  const __nv_bfloat16* b3 = W3 + (long long)nin * H;
-  const int total = a.nbf * a.nbatch;
-  const int F = kGhostFaces;
-  for (int g0 = blockIdx.x * F; g0 < total; g0 += gridDim.x * F) {
-    __syncthreads();
-    // features: one thread per (face, node)
-    for (int i = tid; i < F * a.NpF; i += blockDim.x) {
-      const int fl = i / a.NpF, fi = i - fl * a.NpF;
-      const int gi = g0 + fl;
-      float x[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      if (gi < total) {
-        const int b = gi / a.nbf, g = gi - b * a.nbf;
-        const int e = a.bf_elem[g], f = a.bf_face[g];
-        const float* geo = a.geo + (long long)e * GEO_STRIDE;
-        const long long node = (long long)e * a.Np + a.pat[f * a.NpF + fi];
-        const float* qb = a.q + (long long)b * 9 * a.ldq + node;
-        float q[9];
-        for (int c = 0; c < 9; ++c) q[c] = qb[c * a.ldq];
-        face_features(q, geo + G_N + 3 * f, geo + G_S + 3 * f, geo + G_T + 3 * f, geo[G_IZP],
-                      geo[G_IZP] / geo[G_IZS], x);
-      }
-      for (int c = 0; c < 9; ++c) sx[(fi * 9 + c) * F + fl] = x[c];
-    }
-    __syncthreads();
-    if (tid < F) {
-      float ss = 0.f;
-      for (int k = 0; k < nin; ++k) ss += sx[k * F + tid] * sx[k * F + tid];
-      sr[tid] = sqrtf(ss / nin);
-    }
-    __syncthreads();
-    for (int i = tid; i < nin * F; i += blockDim.x) {
-      const float r = sr[i % F];
-      sx[i] = r > 0.f ? sx[i] / r : 0.f;
-    }
-    __syncthreads();
-    // dense layers: out[j][f] = act(sum_k W[j][k] in[k][f] + b[j]), 8 faces per thread
-    auto layer = [&](const __nv_bfloat16* W, const __nv_bfloat16* bias, const float* in, int kin, float* out,
-                     int nout, bool act) {
-      for (int j2 = tid; j2 < 2 * nout; j2 += blockDim.x) {
-        const int j = j2 >> 1, h = (j2 & 1) * 8;
-        float acc[8];
-        const float bj = __bfloat162float(bias[j]);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) acc[u] = bj;
-        const __nv_bfloat16* wr = W + (long long)j * kin;
-        for (int k = 0; k < kin; ++k) {
-          const float w = __bfloat162float(wr[k]);
-          const float4 x0 = *reinterpret_cast<const float4*>(in + k * F + h);
-          const float4 x1 = *reinterpret_cast<const float4*>(in + k * F + h + 4);
-          acc[0] = fmaf(w, x0.x, acc[0]);
-          acc[1] = fmaf(w, x0.y, acc[1]);
-          acc[2] = fmaf(w, x0.z, acc[2]);
-          acc[3] = fmaf(w, x0.w, acc[3]);
-          acc[4] = fmaf(w, x1.x, acc[4]);
-          acc[5] = fmaf(w, x1.y, acc[5]);
-          acc[6] = fmaf(w, x1.z, acc[6]);
-          acc[7] = fmaf(w, x1.w, acc[7]);
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) out[j * F + h + u] = act ? gelu(acc[u]) : acc[u];
-      }
-    };
-    layer(W1, b1, sx, nin, sh1, H, true);
-    __syncthreads();
-    layer(W2, b2, sh1, H, sh2, H, true);
-    __syncthreads();
-    layer(W3, b3, sh2, H, sy, nin, false);
-    __syncthreads();
-    for (int i = tid; i < F * a.NpF; i += blockDim.x) {
-      const int fl = i / a.NpF, fi = i - fl * a.NpF;
-      const int gi = g0 + fl;
-      if (gi >= total) continue;
-      const int b = gi / a.nbf, g = gi - b * a.nbf;
-      const int e = a.bf_elem[g], f = a.bf_face[g];
-      const float* geo = a.geo + (long long)e * GEO_STRIDE;
-      // incoming values of the prediction, clamped by the outgoing values of the trace
-      const float* x = sx + fi * 9 * F + fl;
-      const float* y = sy + fi * 9 * F + fl;
-      const float r = sr[fl] / geo[G_IZP];  // RMS scale times Zp
-      float w[3];
-      for (int k = 0; k < 3; ++k) {
-        const float bnd = a.rho_max * fabsf(x[(3 + k) * F]);
-        w[k] = r * fminf(fmaxf(y[k * F], -bnd), bnd);
-      }
-      // ghost: traction w0 n + w1 s + w2 t, zero velocity
-      const float* n = geo + G_N + 3 * f;
-      const float* s = geo + G_S + 3 * f;
-      const float* t = geo + G_T + 3 * f;
-      float q[9];
-      // S = w0 n n + w1 (n s + s n) + w2 (n t + t n): S n = w0 n + w1 s + w2 t (n.n = 1, s.n = t.n = 0)
-      auto comp = [&](int p, int q2) {
-        return w[0] * n[p] * n[q2] + w[1] * (n[p] * s[q2] + s[p] * n[q2]) + w[2] * (n[p] * t[q2] + t[p] * n[q2]);
-      };
-      q[0] = comp(0, 0);
-      q[1] = comp(1, 1);
-      q[2] = comp(2, 2);
-      q[3] = comp(0, 1);
-      q[4] = comp(1, 2);
-      q[5] = comp(0, 2);
-      q[6] = q[7] = q[8] = 0.f;
-      float* out = a.ghost + ((long long)b * a.nbf + g) * 9 * a.NpF + fi;
-      for (int c = 0; c < 9; ++c) out[c * a.NpF] = q[c];
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
-// Training (FP32): tiled GEMM C = op(A) op(B) (+ C), elementwise kernels, Adam.
+// Training (FP32): elementwise kernels and Adam (the GEMMs run on the tensor
+// cores, mlp_tc.cuh).
 // ---------------------------------------------------------------------------
-
-// C[M][N] (row stride ldc) = sum_k A(m,k) B(k,n) (+ C when accumulate), where
-// A(m,k) = TA ? A[k*lda + m] : A[m*lda + k] and B(k,n) = TB ? B[n*ldb + k] : B[k*ldb + n].
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
-                                                   const float* __restrict__ B, int ldb, float* C, int ldc,
-                                                   int accumulate) {
-  constexpr int T = 64, KT = 16;
-  __shared__ float sa[KT][T + 4];
-  __shared__ float sb[KT][T + 4];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int m0 = blockIdx.y * T, n0 = blockIdx.x * T;
-  float acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += KT) {
-    for (int i = threadIdx.x; i < KT * T; i += 256) {
-      const int kk = i / T, mm = i - kk * T;
-      const int m = m0 + mm, k = k0 + kk;
-      sa[kk][mm] = (m < M && k < K) ? (TA ? A[(long long)k * lda + m] : A[(long long)m * lda + k]) : 0.f;
-      const int n = n0 + mm;
-      sb[kk][mm] = (n < N && k < K) ? (TB ? B[(long long)n * ldb + k] : B[(long long)k * ldb + n]) : 0.f;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < KT; ++kk) {
-      float av[4], bv[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        av[u] = sa[kk][ty + 16 * u];
-        bv[u] = sb[kk][tx + 16 * u];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int m = m0 + ty + 16 * u, n = n0 + tx + 16 * v;
-      if (m < M && n < N) {
-        float* c = C + (long long)m * ldc + n;
-        *c = accumulate ? *c + acc[u][v] : acc[u][v];
-      }
-    }
-}
 
 // z[b][j] += bias[j]; a = gelu(z) (act) or a = z.
 __global__ void bias_act_kernel(int rows, int cols, float* z, const float* bias, float* a, int act) {

@@ -24,6 +24,8 @@
 #include "group_kernel.cuh"
 #include "boundary_mlp.cuh"
 #include "halo.cuh"
+#include "mlp_tc.cuh"
+#include "boundary_tc.cuh"
 
 #include <unistd.h>
 
@@ -127,6 +129,7 @@ struct nexd_ctx {
   float mlp_rho = 0.f;               // bound of the incoming / outgoing characteristic ratio
   int ghost_grid = 0;
   size_t ghost_smem = 0;
+  uint4* mlp_wimg = nullptr;         // the network's weight images for the tensor cores
   // movie: nodal displacement and per-element frames (src/timeloopMod.f90:482-489, 576-581)
   int movie_frame = 0, movie_max = 0, movie_last_it = 0;
   float init_value = 0.f;            // start value of every field (the reference's 1e-24)
@@ -998,6 +1001,18 @@ __global__ void set_step_kernel(int* it_dev, int it) {
 
 // Enqueues `nsteps` steps on the context's stream; the step number comes from
 // the device counter (set before, advanced by tick_kernel after each step).
+using GhostTcFn = void (*)(const GhostTcArgs);
+GhostTcFn ghost_tc_fn(int NpF) {
+  switch (NpF) {
+    case 3: return ghost_tc_kernel<3>;
+    case 6: return ghost_tc_kernel<6>;
+    case 10: return ghost_tc_kernel<10>;
+    case 15: return ghost_tc_kernel<15>;
+    case 21: return ghost_tc_kernel<21>;
+    default: return nullptr;
+  }
+}
+
 // Launches the stage kernel of one element class (NPML elements first in the
 // internal order, then the rest) with the kernel kind chosen for it.
 void launch_class(nexd_ctx* c, StageArgs& a, bool pml) {
@@ -1202,8 +1217,9 @@ void enqueue_stage_kernels(nexd_ctx* c, StageArgs& a) {
     ga.w = c->mlp_w;
     ga.rho_max = c->mlp_rho;
     ga.ghost = c->ghost;
+    GhostTcArgs ta{ga, c->mlp_wimg, c->flag};
     const int ev = ev_begin(c, NEXD_K_BOUNDARY);
-    ghost_kernel<<<c->ghost_grid, kGhostThreads, c->ghost_smem, c->stream>>>(ga);
+    ghost_tc_fn(c->NpF)<<<c->ghost_grid, kGhostTcThreads, c->ghost_smem, c->stream>>>(ta);
     ev_end(c, ev);
     ++c->launches;
   }
@@ -1376,7 +1392,7 @@ int finish(nexd_ctx* c) {
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (c->profiling) ev_collect(c);
   if (flag & 4) return set_err(c, NEXD_ERR_TIMEOUT, "halo arrival wait ran out: a neighbour partition did not write its traces");
-  if (flag & 2) return set_err(c, NEXD_ERR_CUDA, "tensor-core completion wait timed out in a stage kernel");
+  if (flag & 2) return set_err(c, NEXD_ERR_CUDA, "tensor-core completion wait timed out (stage or boundary network kernel)");
   if (flag) return set_err(c, NEXD_ERR_NONFINITE, "non-finite value in the wavefield at a receiver");
   return NEXD_OK;
 }
@@ -1686,16 +1702,21 @@ int nexd_set_boundary_mlp(nexd_ctx* c, const float* params, int64_t count, float
     if ((st = dalloc(c, &c->mlp_stage, size_t(count))) || (st = dalloc(c, &c->mlp_w, size_t(count))) ||
         (st = dalloc(c, &c->ghost, size_t(c->nbatch) * c->nbf * 9 * c->NpF)))
       return st;
-    c->ghost_smem = ghost_smem_bytes(nin);
-    CUDA_TRY(c, cudaFuncSetAttribute(ghost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c->ghost_smem)));
+    const GhostTcLayout L = GhostTcLayout::of(nin);
+    GhostTcFn fn = ghost_tc_fn(c->NpF);
+    if (!fn) return set_err(c, NEXD_ERR_UNSUPPORTED, "no boundary network kernel for this order");
+    if ((st = dalloc(c, &c->mlp_wimg, size_t(L.weights() / 16)))) return st;
+    c->ghost_smem = L.smem();
+    CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c->ghost_smem)));
     int per_sm = 0;
-    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ghost_kernel, kGhostThreads, c->ghost_smem));
-    if (per_sm < 1) return set_err(c, NEXD_ERR_UNSUPPORTED, "boundary MLP kernel does not fit on an SM");
-    const long long groups = ((long long)c->nbf * c->nbatch + kGhostFaces - 1) / kGhostFaces;
-    c->ghost_grid = int(std::max<long long>(1, std::min<long long>(groups, (long long)per_sm * c->nsm)));
+    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kGhostTcThreads, c->ghost_smem));
+    if (per_sm < 1) return set_err(c, NEXD_ERR_UNSUPPORTED, "boundary network kernel does not fit on an SM");
+    const long long tiles = ((long long)c->nbf * c->nbatch + 127) / 128;
+    c->ghost_grid = int(std::max<long long>(1, std::min<long long>(tiles, (long long)per_sm * c->nsm)));
   }
   CUDA_TRY(c, cudaMemcpyAsync(c->mlp_stage, params, size_t(count) * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   to_bf16_kernel<<<unsigned((count + 255) / 256), 256, 0, c->stream>>>(count, c->mlp_stage, c->mlp_w);
+  pack_ghost_weights_kernel<<<c->nsm, 256, 0, c->stream>>>(nin, c->mlp_w, reinterpret_cast<unsigned char*>(c->mlp_wimg));
   CUDA_TRY(c, cudaGetLastError());
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->mlp_on = true;
@@ -1779,7 +1800,8 @@ int nexd_get_face_traces(nexd_ctx* c, int32_t nfaces, const int32_t* elem, const
 int64_t nexd_mlp_param_count(int32_t n_in, int32_t n_hidden) { return mlp_param_count(n_in, n_hidden); }
 
 int64_t nexd_mlp_workspace_floats(int32_t n_in, int32_t n_hidden, int32_t batch) {
-  return 6LL * batch * n_hidden + 2LL * batch * n_in + 256;
+  // activations and their gradients, loss partials, split-K partial sums
+  return 6LL * batch * n_hidden + 2LL * batch * n_in + 256 + kMlpSplitFloats;
 }
 
 }  // extern "C"
@@ -1788,7 +1810,7 @@ namespace {
 
 struct MlpView {
   const float *W1, *b1, *W2, *b2, *W3, *b3;
-  float *Z1, *A1, *Z2, *A2, *Y, *dY, *dH1, *dH2, *partial;
+  float *Z1, *A1, *Z2, *A2, *Y, *dY, *dH1, *dH2, *partial, *splitk;
 };
 
 MlpView mlp_view(int nin, int H, int B, const float* p, float* work) {
@@ -1809,29 +1831,49 @@ MlpView mlp_view(int nin, int H, int B, const float* p, float* work) {
   v.dH1 = v.dY + BI;
   v.dH2 = v.dH1 + BH;
   v.partial = v.dH2 + BH;
+  v.splitk = v.partial + 256;
   return v;
 }
 
+// C = op(A) op(B) (+ C) on the tensor cores (mlp_tc.cuh): one CTA per 128
+// rows, K split over CTAs when the rows alone leave SMs idle.
 template <bool TA, bool TB>
 void gemm(cudaStream_t s, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc,
-          int acc) {
-  dim3 grid((N + 63) / 64, (M + 63) / 64);
-  gemm_kernel<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, acc);
+          int acc, float* splitk) {
+  static bool attr = false;  // one instantiation per (TA, TB)
+  if (!attr) {
+    cudaFuncSetAttribute(tc_gemm_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    attr = true;
+  }
+  const int NP = tcg_np(N);
+  const int mt = (M + 127) / 128, nchunk = (K + 63) / 64;
+  int splits = std::min(std::min(kTcgMaxSplits, std::max(1, 148 / mt)), nchunk);
+  while (splits > 1 && (long long)splits * M * N > kMlpSplitFloats) --splits;
+  const int cper = (nchunk + splits - 1) / splits;
+  splits = (nchunk + cper - 1) / cper;  // every split gets at least one chunk
+  TcGemmArgs g{M, N, K, A, lda, B, ldb, C, ldc, acc, cper * 64, splitk};
+  tc_gemm_kernel<TA, TB><<<dim3(mt, splits), kTcgThreads, tcg_smem_bytes(NP, tcg_nbuf(NP)), s>>>(g);
+  if (splits > 1) {
+    const long long n = (long long)M * N;
+    splitk_reduce_kernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(M, N, splits, splitk, C, ldc, acc);
+  }
 }
 
 unsigned blocks_for(long long n) { return unsigned((n + 255) / 256); }
 
 void mlp_forward(cudaStream_t s, int nin, int H, int B, const float* x, const MlpView& v) {
-  gemm<false, true>(s, B, H, nin, x, nin, v.W1, nin, v.Z1, H, 0);
+  gemm<false, true>(s, B, H, nin, x, nin, v.W1, nin, v.Z1, H, 0, v.splitk);
   bias_act_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>(B, H, v.Z1, v.b1, v.A1, 1);
-  gemm<false, true>(s, B, H, H, v.A1, H, v.W2, H, v.Z2, H, 0);
+  gemm<false, true>(s, B, H, H, v.A1, H, v.W2, H, v.Z2, H, 0, v.splitk);
   bias_act_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>(B, H, v.Z2, v.b2, v.A2, 1);
-  gemm<false, true>(s, B, nin, H, v.A2, H, v.W3, H, v.Y, nin, 0);
+  gemm<false, true>(s, B, nin, H, v.A2, H, v.W3, H, v.Y, nin, 0, v.splitk);
   bias_act_kernel<<<blocks_for((long long)B * nin), 256, 0, s>>>(B, nin, v.Y, v.b3, v.Y, 0);
 }
 
 int mlp_check(int32_t n_in, int32_t n_hidden, int32_t batch) {
   if (n_in < 1 || n_hidden < 1 || batch < 1) return set_err(nullptr, NEXD_ERR_INVALID, "bad MLP dimensions");
+  if (n_in > kTcgMaxN || n_hidden > kTcgMaxN)
+    return set_err(nullptr, NEXD_ERR_UNSUPPORTED, "MLP layers wider than 256 are not supported");
   return NEXD_OK;
 }
 
@@ -1873,15 +1915,15 @@ int nexd_mlp_loss_grad(int32_t n_in, int32_t n_hidden, const float* params, cons
   const long long n = (long long)B * nin;
   mse_kernel<<<256, 256, 0, s>>>(n, B, v.Y, target, v.dY, v.partial);
   sum_partials_kernel<<<1, 32, 0, s>>>(256, v.partial, B, loss);
-  gemm<true, false>(s, nin, H, B, v.dY, nin, v.A2, H, gW3, H, 0);
+  gemm<true, false>(s, nin, H, B, v.dY, nin, v.A2, H, gW3, H, 0, v.splitk);
   colsum_kernel<<<blocks_for(nin), 256, 0, s>>>(B, nin, v.dY, gb3);
-  gemm<false, false>(s, B, H, nin, v.dY, nin, v.W3, H, v.dH2, H, 0);
+  gemm<false, false>(s, B, H, nin, v.dY, nin, v.W3, H, v.dH2, H, 0, v.splitk);
   gelu_back_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>((long long)B * H, v.dH2, v.Z2);
-  gemm<true, false>(s, H, H, B, v.dH2, H, v.A1, H, gW2, H, 0);
+  gemm<true, false>(s, H, H, B, v.dH2, H, v.A1, H, gW2, H, 0, v.splitk);
   colsum_kernel<<<blocks_for(H), 256, 0, s>>>(B, H, v.dH2, gb2);
-  gemm<false, false>(s, B, H, H, v.dH2, H, v.W2, H, v.dH1, H, 0);
+  gemm<false, false>(s, B, H, H, v.dH2, H, v.W2, H, v.dH1, H, 0, v.splitk);
   gelu_back_kernel<<<blocks_for((long long)B * H), 256, 0, s>>>((long long)B * H, v.dH1, v.Z1);
-  gemm<true, false>(s, H, nin, B, v.dH1, H, x, nin, gW1, nin, 0);
+  gemm<true, false>(s, H, nin, B, v.dH1, H, x, nin, gW1, nin, 0, v.splitk);
   colsum_kernel<<<blocks_for(H), 256, 0, s>>>(B, H, v.dH1, gb1);
   return mlp_status();
 }

@@ -4,8 +4,9 @@ against the same network evaluated on the host, the zero-output network
 against the plain absorbing boundary, and a trained network against the plain
 boundary on a held-out source, both judged by the wide-NPML run.
 
-Tolerances: gradients and outputs of the FP32 training kernels within 1e-4
-relative L2 of FP64; the ghost kernel (BF16 weights, FP32 accumulation)
+Tolerances: gradients and outputs of the training kernels (tcgen05 GEMMs
+with three-way split BF16 operands, FP32 accumulation; FP32 elementwise
+kernels) within 1e-4 relative L2 of FP64; the ghost kernel (BF16 weights, FP32 accumulation)
 within 1e-4 of the host evaluation with the same BF16 weights.
 """
 import ctypes as C
@@ -74,6 +75,40 @@ def test_mlp_kernels_match_oracle():
     gg = g32.cpu().numpy().astype(np.float64)
     p1 = p - 1e-3 * gg / (np.abs(gg) + 1e-8)
     assert np.allclose(tr.params.cpu().numpy(), p1, rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("nin,B", [(54, 300), (135, 4096), (189, 2048)])
+def test_mlp_tensor_core_gemms_at_training_size(nin, B):
+    """The training GEMMs on tcgen05 (split-BF16 operands, FP32 accumulation)
+    at the trainer's batch size, where the weight gradients split K over
+    CTAs, and for the widest layer (189 = 9 x 21 face values, one staging
+    buffer): loss, gradients and forward within the FP32 tolerances of the
+    FP64 oracle."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(nin)
+    p = boundary.init_params(nin, H, seed=5)
+    W1, b1, W2, b2, W3, b3 = mlp_oracle.unpack(p, nin, H)
+    p = np.concatenate([W1.ravel(), rng.standard_normal(H) * 0.1, W2.ravel(), rng.standard_normal(H) * 0.1,
+                        rng.standard_normal(nin * H) * 0.3 / np.sqrt(H), rng.standard_normal(nin) * 0.05])
+    p = p.astype(np.float32)
+    x = rng.standard_normal((B, nin)).astype(np.float32)
+    t = rng.standard_normal((B, nin)).astype(np.float32)
+    tr = boundary.Trainer(nin, params=p, batch=B)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    tr.loss_grad(xd, td)
+    torch.cuda.synchronize()
+    loss_ref, g_ref = mlp_oracle.loss_grad(p, x, t, nin, H)
+    assert abs(float(tr.loss[0]) - loss_ref) / loss_ref < 1e-5
+    g = tr.grads.cpu().numpy().astype(np.float64)
+    o = 0
+    for n in (H * nin, H, H * H, H, nin * H, nin):
+        assert rel_l2(g[o:o + n], g_ref[o:o + n]) < 1e-4
+        o += n
+    y = torch.zeros((B, nin), dtype=torch.float32, device="cuda")
+    lib = _abi.gpu_lib()
+    assert lib.nexd_mlp_forward(nin, H, tr._ptr(tr.params), tr._ptr(xd), B, tr._ptr(y), tr._ptr(tr.work), None) == 0
+    y_ref, _ = mlp_oracle.forward(p.astype(np.float64), x.astype(np.float64), nin, H)
+    assert rel_l2(y.cpu().numpy(), y_ref) < 1e-5
 
 
 def _absorbing_cube(tmp_path, nt=20):
