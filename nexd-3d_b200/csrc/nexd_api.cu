@@ -1350,11 +1350,21 @@ int enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
     drop_graphs(c);
     c->graph_energy = c->energy_on;
   }
+  // LSERK4 and Euler flip the buffer parity every step (an odd number of
+  // stages), so runs start at either parity: the graphs of both are captured
+  // the first time one is needed, so that no later run pays for a capture
+  const bool flips = (c->timeint == 4 || c->timeint == 1) && (c->nstage & 1);
   const int p = c->cur;
   if (n >= 2) {
-    if (!c->gexec[p]) {
-      if (int st = capture_steps(c, 2, &c->gexec[p], &c->graph_launches)) return st;
-      if (c->cur != p) return set_err(c, NEXD_ERR_CUDA, "two-step graph changed the buffer parity");
+    for (int k = 0; k < (flips ? 2 : 1); ++k) {
+      const int q = k == 0 ? p : 1 - p;
+      if (c->gexec[q]) continue;
+      c->cur = q;
+      const int st = capture_steps(c, 2, &c->gexec[q], &c->graph_launches);
+      const int end = c->cur;
+      c->cur = p;
+      if (st) return st;
+      if (end != q) return set_err(c, NEXD_ERR_CUDA, "two-step graph changed the buffer parity");
     }
     for (; n >= 2; n -= 2) {
       CUDA_TRY(c, cudaGraphLaunch(c->gexec[p], c->stream));
@@ -1363,10 +1373,14 @@ int enqueue_steps(nexd_ctx* c, int it_begin, int it_end) {
   }
   if (n == 1) {
     const int q = c->cur;
-    if (!c->gexec1[q]) {
-      if (int st = capture_steps(c, 1, &c->gexec1[q], &c->graph1_launches[q])) return st;
-      c->gend1[q] = c->cur;  // capture advanced the host-side buffer index
+    for (int k = 0; k < (flips ? 2 : 1); ++k) {
+      const int r = k == 0 ? q : 1 - q;
+      if (c->gexec1[r]) continue;
+      c->cur = r;
+      const int st = capture_steps(c, 1, &c->gexec1[r], &c->graph1_launches[r]);
+      c->gend1[r] = c->cur;  // capture advanced the host-side buffer index
       c->cur = q;
+      if (st) return st;
     }
     CUDA_TRY(c, cudaGraphLaunch(c->gexec1[q], c->stream));
     c->launches += c->graph1_launches[q];
@@ -1947,6 +1961,7 @@ struct nexd_group {
   cudaEvent_t fork = nullptr, span[2] = {nullptr, nullptr};
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec_flip = nullptr;  // the same two steps from the other buffer parity
   std::vector<int> parity;       // members' buffer parity when the graph was captured
   std::vector<int> graph_launches;
   float span_ms = 0.f;
@@ -1973,10 +1988,19 @@ int gerr(nexd_group* g, int code, const std::string& msg) {
   } while (0)
 
 void drop_group_graph(nexd_group* g) {
-  if (g->gexec) {
-    cudaGraphExecDestroy(g->gexec);
-    g->gexec = nullptr;
-  }
+  for (cudaGraphExec_t* x : {&g->gexec, &g->gexec_flip})
+    if (*x) {
+      cudaGraphExecDestroy(*x);
+      *x = nullptr;
+    }
+}
+
+// Every member flips its buffer parity each step (LSERK4 and Euler: an odd
+// number of stages), so runs start at either parity.
+bool members_flip(const nexd_group* g) {
+  for (const nexd_ctx* c : g->m)
+    if (!((c->timeint == 4 || c->timeint == 1) && (c->nstage & 1))) return false;
+  return true;
 }
 
 // Members' work forked from the group stream and joined back: `body` enqueues
@@ -1996,8 +2020,8 @@ int fork_join(nexd_group* g, F body) {
 
 void enqueue_group_persistent(nexd_group* g, int nsteps);
 
-int capture_group(nexd_group* g) {
-  drop_group_graph(g);
+// Captures two steps of every member from their current buffers into *exec.
+int capture_group_once(nexd_group* g, cudaGraphExec_t* exec) {
   cudaGraph_t graph = nullptr;
   GCUDA(g, cudaStreamBeginCapture(g->s, cudaStreamCaptureModeThreadLocal));
   std::vector<int64_t> before(g->m.size());
@@ -2019,10 +2043,25 @@ int capture_group(nexd_group* g) {
   }
   if (st) return st;
   if (e != cudaSuccess) return gerr(g, NEXD_ERR_CUDA, std::string("group capture: ") + cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&g->gexec, graph, 0);
+  e = cudaGraphInstantiate(exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return gerr(g, NEXD_ERR_CUDA, std::string("group instantiate: ") + cudaGetErrorString(e));
   return NEXD_OK;
+}
+
+// The group's two-step graph from the members' current buffers and, when
+// every member flips parity each step, the one from the other parity too, so
+// that no later run pays for a capture.
+int capture_group(nexd_group* g) {
+  drop_group_graph(g);
+  if (int st = capture_group_once(g, &g->gexec)) return st;
+  if (!members_flip(g)) return NEXD_OK;
+  std::vector<int> base = g->parity;
+  for (size_t i = 0; i < g->m.size(); ++i) g->m[i]->cur = 1 - base[i];
+  const int st = capture_group_once(g, &g->gexec_flip);
+  for (size_t i = 0; i < g->m.size(); ++i) g->m[i]->cur = base[i];
+  g->parity = base;
+  return st;
 }
 
 // Mode 1 covers groups of at most kGroupMax members that all step with LSERK4
@@ -2182,12 +2221,18 @@ int nexd_group_run(nexd_group* g, int32_t it_begin, int32_t it_end) {
   }
   int n = it_end - it_begin + 1;
   if (n >= 2) {
-    bool stale = !g->gexec;
-    for (size_t i = 0; i < g->m.size(); ++i) stale |= g->parity[i] != g->m[i]->cur;
-    if (stale)
+    bool same = g->gexec != nullptr, flipped = g->gexec_flip != nullptr;
+    for (size_t i = 0; i < g->m.size(); ++i) {
+      same = same && g->parity[i] == g->m[i]->cur;
+      flipped = flipped && g->parity[i] == 1 - g->m[i]->cur;
+    }
+    if (!same && !flipped) {
       if (int st = capture_group(g)) return st;
+      same = true;
+    }
+    cudaGraphExec_t x = same ? g->gexec : g->gexec_flip;
     for (; n >= 2; n -= 2) {
-      GCUDA(g, cudaGraphLaunch(g->gexec, g->s));
+      GCUDA(g, cudaGraphLaunch(x, g->s));
       for (size_t i = 0; i < g->m.size(); ++i) g->m[i]->launches += g->graph_launches[i];
     }
   }
