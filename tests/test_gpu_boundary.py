@@ -2,7 +2,7 @@
 kernels against the FP64 oracle (oracle/mlp_oracle.py), the ghost-state kernel
 against the same network evaluated on the host, the zero-output network
 against the plain absorbing boundary, and a trained network against the plain
-boundary on a held-out source, both judged by the wide-NPML run.
+boundary on a held-out source, both scored against the wide-NPML run.
 
 Tolerances: gradients and outputs of the training kernels (tcgen05 GEMMs
 with three-way split BF16 operands, FP32 accumulation; FP32 elementwise
