@@ -49,7 +49,7 @@ struct Order {
   static constexpr int CS = 34;           // contravariant-flux row stride (PML): r 0..9, s 10..19, t 20..29
   // shared-memory section sizes in floats, each a multiple of 4 (float4 alignment)
   static constexpr int r4(int x) { return (x + 3) / 4 * 4; }
-  static constexpr int SD = r4(3 * Np * Np);  // Dr, Ds, Dt as [d][k][n]
+  static constexpr int SD = r4(3 * Np * Np);  // Dr, Ds, Dt (each kernel stages its own layout)
   static constexpr int NPAIR = (NpF + 1) / 2;  // face-node pairs per face (last one zero-padded when NpF is odd)
   static constexpr int NFP = 4 * 2 * NPAIR;     // padded face nodes per element
   static constexpr int SL = 4 * NPAIR * Np * 2; // LIFT as [face][pair][n][2]
@@ -607,7 +607,7 @@ template <int N, bool ATT, bool PML, int MODE>
 __device__ __forceinline__ void stage_body(const StageArgs& a, int w0, int wstep, float* smem) {
   using O = Order<N>;
   constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, QS = O::QS, CS = O::CS;
-  float* sD = smem;              // 3*Np*Np: D[d][k][n]
+  float* sD = smem;              // (Dr, Ds) pairs [k][n], then Dt [k][n]
   float* sL = sD + O::SD;        // LIFT in face-node pairs
   float* sBuf = sL + O::SL;      // 2 prefetch buffers
   float* sQI = sBuf + 2 * O::BUF;  // non-PML: interleaved own wavefield [e][k][QS]
@@ -616,7 +616,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int w0, int wstep
   unsigned char* sPat = reinterpret_cast<unsigned char*>(sAmp + O::SAMP);  // face patterns
 
   const int tid = threadIdx.x;
-  for (int i = tid; i < 3 * Np * Np; i += blockDim.x) sD[i] = a.D[i];
+  // Dr and Ds of a (k, node) as one 8-byte pair, then Dt
+  for (int i = tid; i < Np * Np; i += blockDim.x) {
+    reinterpret_cast<float2*>(sD)[i] = make_float2(a.D[i], a.D[Np * Np + i]);
+    sD[2 * Np * Np + i] = a.D[2 * Np * Np + i];
+  }
   for (int i = tid; i < O::SL; i += blockDim.x) sL[i] = a.L[i];
   if (NpF & 1)  // padding slots of the amplitude pairs stay zero
     for (int i = tid; i < E * 3 * 4; i += blockDim.x)
@@ -740,7 +744,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int w0, int wstep
         sv[i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
         t[i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
       }
-      r[9] = sv[9] = t[9] = 0.f;
+      // the pad slot of each row carries one velocity component (read with
+      // field 8 of the row as one 8-byte load in the volume loop)
+      r[9] = ATT ? qv[6] : 0.f;
+      sv[9] = ATT ? qv[7] : 0.f;
+      t[9] = ATT ? qv[8] : 0.f;
 #pragma unroll
       for (int j = 0; j < 5; ++j) {
         cf[j] = make_float2(r[2 * j], r[2 * j + 1]);
@@ -766,7 +774,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int w0, int wstep
       const float* qe = sQI + le * O::QE;
 #pragma unroll
       for (int k = 0; k < Np; ++k) {
-        const float dx = sD[k * Np + n], dy = sD[Np * Np + k * Np + n], dz = sD[2 * Np * Np + k * Np + n];
+        const float2 drs = reinterpret_cast<const float2*>(sD)[k * Np + n];
+        const float dx = drs.x, dy = drs.y, dz = sD[2 * Np * Np + k * Np + n];
         const float2 d0 = make_float2(dx, dx), d1 = make_float2(dy, dy), d2 = make_float2(dz, dz);
         const float4 qa = ld4(qe + k * QS), qb = ld4(qe + k * QS + 4);
         const float q8 = qe[k * QS + 8];
@@ -819,26 +828,26 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int w0, int wstep
     } else {
 #pragma unroll
       for (int c = 0; c < 9; ++c) rq[c] = 0.f;
-      float2 acc[4];  // fields 0..7 in pairs; field 8 as 4-byte loads (its pair's second word is padding)
+      float2 acc[4];  // fields 0..7 in pairs; field 8 (its pair's second word is a velocity component)
       float acc8 = 0.f;
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[j] = make_float2(0.f, 0.f);
       float2 v01r = make_float2(0.f, 0.f), v01s = v01r, v01t = v01r;
       float v2r = 0.f, v2s = 0.f, v2t = 0.f;
       const float* cfe = sCF + le * O::CFE;
-      const float* qv = sQF + le * Np;
 #pragma unroll 5
       for (int k = 0; k < Np; ++k) {
-        const float4 d = make_float4(sD[k * Np + n], sD[Np * Np + k * Np + n], sD[2 * Np * Np + k * Np + n], 0.f);
+        const float2 drs = reinterpret_cast<const float2*>(sD)[k * Np + n];
+        const float4 d = make_float4(drs.x, drs.y, sD[2 * Np * Np + k * Np + n], 0.f);
         const float2 d0 = make_float2(d.x, d.x), d1 = make_float2(d.y, d.y), d2 = make_float2(d.z, d.z);
         const float2* cf = reinterpret_cast<const float2*>(cfe + k * CS);
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[j] = __ffma2_rn(d0, cf[j], __ffma2_rn(d1, cf[5 + j], __ffma2_rn(d2, cf[10 + j], acc[j])));
-        const float* c8 = cfe + k * CS + 8;
-        acc8 = fmaf(d.x, c8[0], fmaf(d.y, c8[10], fmaf(d.z, c8[20], acc8)));
+        const float2 pr8 = cf[4], ps8 = cf[9], pt8 = cf[14];  // (field 8, velocity component)
+        acc8 = fmaf(d.x, pr8.x, fmaf(d.y, ps8.x, fmaf(d.z, pt8.x, acc8)));
         if (ATT) {
-          const float2 v01 = make_float2(qv[6 * O::QF + k], qv[7 * O::QF + k]);
-          const float v2 = qv[8 * O::QF + k];
+          const float2 v01 = make_float2(pr8.y, ps8.y);
+          const float v2 = pt8.y;
           v01r = __ffma2_rn(d0, v01, v01r);
           v01s = __ffma2_rn(d1, v01, v01s);
           v01t = __ffma2_rn(d2, v01, v01t);
