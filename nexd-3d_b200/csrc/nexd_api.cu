@@ -20,7 +20,7 @@
 #include "stage_kernel.cuh"
 #include "stage_tc.cuh"
 #include "stage_pair.cuh"
-#include "stage_npml_split.cuh"
+#include "stage_npml_bulk.cuh"
 #include "group_kernel.cuh"
 #include "boundary_mlp.cuh"
 #include "halo.cuh"
@@ -332,32 +332,35 @@ KernelFn pick_pair_kernel(int N, bool att, int mode, size_t& smem) {
 }
 
 // Kernel kinds per element class: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3,
-// the node-pair FP32 kernel (elements outside the NPML) and the NPML kernel
-// with two threads per node (NPML elements); the last two give the same
-// results as NEXD_CONTRACT_FP32 and are chosen by the autotune or pinned.
+// the node-pair FP32 kernel (elements outside the NPML) and the FP32 NPML
+// kernel whose element-local state arrives by bulk copies (NPML elements);
+// the last two give the same results as NEXD_CONTRACT_FP32 and are chosen
+// by the autotune or pinned.
 constexpr int KIND_FP32_PAIRS = 2;
-constexpr int KIND_NPML_SPLIT = 3;
+constexpr int KIND_NPML_BULK = 3;
 constexpr int NKINDS = 4;
 
 template <int N>
-KernelFn pick_split(bool att, int mode) {
-  if (mode == MODE_LSERK) return att ? stage_npml_split_kernel<N, true, MODE_LSERK> : stage_npml_split_kernel<N, false, MODE_LSERK>;
-  return att ? stage_npml_split_kernel<N, true, MODE_TVD> : stage_npml_split_kernel<N, false, MODE_TVD>;
+KernelFn pick_bulk(bool att, int mode) {
+  if (mode == MODE_LSERK) return att ? stage_npml_bulk_kernel<N, true, MODE_LSERK> : stage_npml_bulk_kernel<N, false, MODE_LSERK>;
+  return att ? stage_npml_bulk_kernel<N, true, MODE_TVD> : stage_npml_bulk_kernel<N, false, MODE_TVD>;
 }
 
-// The NPML kernel with two threads per node (512-thread blocks; orders 2-5).
-KernelFn pick_split_kernel(int N, bool att, int mode, size_t& smem) {
+// Orders whose bulk-staged NPML kernel fits the 227 KB of shared memory a
+// block can have: 3 and 4 (orders 2 and 5 need 231 and 236 KB).
+bool bulk_order_supported(int N) { return N == 3 || N == 4; }
+
+// The FP32 NPML kernel with bulk-copied element-local state.
+KernelFn pick_bulk_kernel(int N, bool att, int mode, size_t& smem) {
   switch (N) {
-    case 2: smem = size_t(SplitOrder<2>::smem_floats()) * 4; return pick_split<2>(att, mode);
-    case 3: smem = size_t(SplitOrder<3>::smem_floats()) * 4; return pick_split<3>(att, mode);
-    case 4: smem = size_t(SplitOrder<4>::smem_floats()) * 4; return pick_split<4>(att, mode);
-    case 5: smem = size_t(SplitOrder<5>::smem_floats()) * 4; return pick_split<5>(att, mode);
+    case 3: smem = size_t(BulkOrder<3>::smem_floats()) * 4; return pick_bulk<3>(att, mode);
+    case 4: smem = size_t(BulkOrder<4>::smem_floats()) * 4; return pick_bulk<4>(att, mode);
     default: smem = 0; return nullptr;
   }
 }
 
 // Threads per block of a kernel kind.
-int kind_threads(int kind) { return kind == KIND_NPML_SPLIT ? 512 : 256; }
+int kind_threads(int) { return 256; }
 
 int elements_per_chunk(int N) {
   const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
@@ -499,8 +502,8 @@ int configure_launch(nexd_ctx* c) {
     } else if (c->kind[which] == KIND_FP32_PAIRS && !pmlk) {
       fn = reinterpret_cast<const void*>(pick_pair_kernel(c->N, c->att, mode, smem));
       E *= 2;
-    } else if (c->kind[which] == KIND_NPML_SPLIT && pmlk) {
-      fn = reinterpret_cast<const void*>(pick_split_kernel(c->N, c->att, mode, smem));
+    } else if (c->kind[which] == KIND_NPML_BULK && pmlk) {
+      fn = reinterpret_cast<const void*>(pick_bulk_kernel(c->N, c->att, mode, smem));
     } else {
       fn = reinterpret_cast<const void*>(pick_kernel(c->N, c->att, pmlk, mode, smem));
     }
@@ -692,7 +695,9 @@ int create_impl(const nexd_desc* d, const nexd_halo_desc* h, nexd_ctx** out) {
   }
   std::vector<float> h_prof;
   if (c->pml && c->Kpml > 0) {
-    h_prof.assign(size_t(c->Kpml) * 9 * Np, 0.f);
+    // 4 floats of slack after the last element: the bulk-copy NPML kernel
+    // copies a chunk's profiles widened to 16-byte boundaries
+    h_prof.assign(size_t(c->Kpml) * 9 * Np + 4, 0.f);
     const size_t ng = size_t(K) * Np;
     for (int ni = 0; ni < c->Kpml; ++ni) {
       const int e = c->new2old[ni];
@@ -776,8 +781,10 @@ int create_impl(const nexd_desc* d, const nexd_halo_desc* h, nexd_ctx** out) {
   }
   const int nq = (c->timeint == 3) ? 3 : 2;
   for (int i = 0; i < nq; ++i) {
-    if ((st = dalloc(c, &c->qbuf[i], size_t(nb) * 9 * c->ldq))) return fail(st);
-    if ((st = fill(c, c->qbuf[i], size_t(nb) * 9 * c->ldq, float(d->init_value)))) return fail(st);
+    // + 4 floats of slack: the bulk-copy NPML kernel reads a chunk's rows
+    // widened to 16-byte boundaries (TVD step-start wavefield)
+    if ((st = dalloc(c, &c->qbuf[i], size_t(nb) * 9 * c->ldq + 4))) return fail(st);
+    if ((st = fill(c, c->qbuf[i], size_t(nb) * 9 * c->ldq + 4, float(d->init_value)))) return fail(st);
     c->init_value = float(d->init_value);
   }
   if (h) {
@@ -813,18 +820,20 @@ int create_impl(const nexd_desc* d, const nexd_halo_desc* h, nexd_ctx** out) {
     }
   }
   if (c->timeint == 4) {
-    if ((st = dalloc(c, &c->res, size_t(nb) * 9 * c->ldq))) return fail(st);
-    CUDA_TRY(c, cudaMemset(c->res, 0, size_t(nb) * 9 * c->ldq * sizeof(float)));
+    if ((st = dalloc(c, &c->res, size_t(nb) * 9 * c->ldq + 4))) return fail(st);  // + slack, as above
+    CUDA_TRY(c, cudaMemset(c->res, 0, (size_t(nb) * 9 * c->ldq + 4) * sizeof(float)));
   }
   if (c->att) {
-    const size_t n = size_t(nb) * 6 * c->nMB * c->ldt;
+    const size_t n = size_t(nb) * 6 * c->nMB * c->ldt + 4;  // + slack, as above
     if ((st = dalloc(c, &c->th, n)) || (st = dalloc(c, &c->th2, n))) return fail(st);
     if ((st = fill(c, c->th, n, float(d->init_value)))) return fail(st);
     CUDA_TRY(c, cudaMemset(c->th2, 0, n * sizeof(float)));
     if ((st = upload(c, &c->ael, h_ael)) || (st = upload(c, &c->wl, h_wl))) return fail(st);
   }
   if (c->pml && c->Kpml > 0) {
-    const size_t n = size_t(nb) * 27 * c->lda;
+    // + 4 floats of slack: the bulk-copy NPML kernel copies a chunk's
+    // auxiliaries widened to 16-byte boundaries
+    const size_t n = size_t(nb) * 27 * c->lda + 4;
     if ((st = dalloc(c, &c->aux, n)) || (st = dalloc(c, &c->aux2, n))) return fail(st);
     CUDA_TRY(c, cudaMemset(c->aux, 0, n * sizeof(float)));
     CUDA_TRY(c, cudaMemset(c->aux2, 0, n * sizeof(float)));
@@ -1029,9 +1038,9 @@ void launch_class(nexd_ctx* c, StageArgs& a, bool pml) {
   } else if (c->kind[cls] == KIND_FP32_PAIRS && !pml) {
     KernelFn f = pick_pair_kernel(c->N, c->att, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);
-  } else if (c->kind[cls] == KIND_NPML_SPLIT && pml) {
-    KernelFn f = pick_split_kernel(c->N, c->att, mode, smem);
-    f<<<grid, 512, sm, c->stream>>>(a);
+  } else if (c->kind[cls] == KIND_NPML_BULK && pml) {
+    KernelFn f = pick_bulk_kernel(c->N, c->att, mode, smem);
+    f<<<grid, 256, sm, c->stream>>>(a);
   } else {
     KernelFn f = pick_kernel(c->N, c->att, pml, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);
@@ -1407,6 +1416,7 @@ int finish(nexd_ctx* c) {
   if (c->profiling) ev_collect(c);
   if (flag & 4) return set_err(c, NEXD_ERR_TIMEOUT, "halo arrival wait ran out: a neighbour partition did not write its traces");
   if (flag & 2) return set_err(c, NEXD_ERR_CUDA, "tensor-core completion wait timed out (stage or boundary network kernel)");
+  if (flag & 8) return set_err(c, NEXD_ERR_CUDA, "bulk-copy completion wait timed out (NPML stage kernel)");
   if (flag) return set_err(c, NEXD_ERR_NONFINITE, "non-finite value in the wavefield at a receiver");
   return NEXD_OK;
 }
@@ -1501,8 +1511,8 @@ int time_class(nexd_ctx* c, bool pml, int reps, float& ms) {
 // Picks, per element class, the fastest on this mesh of the FP32 CUDA-core
 // kernel, the tensor-core kernel (order 4; FP32-accurate, agrees with the
 // FP32 kernel to FP32 rounding, not bit for bit) and the FP32 variants with
-// the same results: the node-pair kernel outside the NPML, the kernel with
-// two threads per node on NPML elements (orders 2-5).
+// the same results: the node-pair kernel outside the NPML (orders 2-5), the
+// kernel with bulk-copied element-local state on NPML elements (orders 3, 4).
 int autotune(nexd_ctx* c) {
   if (int st = finish(c)) return st;  // at a step boundary
   for (int cls = 0; cls < 2; ++cls) {
@@ -1512,7 +1522,7 @@ int autotune(nexd_ctx* c) {
     for (int k = 0; k < NKINDS; ++k) {
       if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N)) continue;
       if (k == KIND_FP32_PAIRS && (cls == 0 || c->N < 2 || c->N > 5)) continue;
-      if (k == KIND_NPML_SPLIT && (cls == 1 || c->N < 2 || c->N > 5)) continue;
+      if (k == KIND_NPML_BULK && (cls == 1 || !bulk_order_supported(c->N))) continue;
       c->kind[cls] = k;
       if (int st = configure_launch(c)) return st;
       if (int st = time_class(c, cls == 0, 3, c->tune_ms[cls][k])) return st;
@@ -1562,10 +1572,10 @@ int nexd_set_contraction_kinds(nexd_ctx* c, const int32_t* kinds) {
   for (int cls = 0; cls < 2; ++cls) {
     const int k = kinds[cls];
     if (k != NEXD_CONTRACT_FP32 && k != NEXD_CONTRACT_BF16X3 && !(cls == 1 && k == KIND_FP32_PAIRS) &&
-        !(cls == 0 && k == KIND_NPML_SPLIT))
+        !(cls == 0 && k == KIND_NPML_BULK))
       return set_err(c, NEXD_ERR_INVALID, "unknown kernel kind for this element class");
-    if (k == KIND_NPML_SPLIT && (c->N < 2 || c->N > 5))
-      return set_err(c, NEXD_ERR_UNSUPPORTED, "the two-threads-per-node NPML kernel covers orders 2 to 5");
+    if (k == KIND_NPML_BULK && !bulk_order_supported(c->N))
+      return set_err(c, NEXD_ERR_UNSUPPORTED, "the bulk-copy NPML kernel covers orders 3 and 4");
     if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N))
       return set_err(c, NEXD_ERR_UNSUPPORTED, "the tensor-core contraction covers order 4");
     if (k == KIND_FP32_PAIRS && (c->N < 2 || c->N > 5))

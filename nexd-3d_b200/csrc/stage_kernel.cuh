@@ -160,7 +160,8 @@ struct StageArgs {
   int nslot;
   int last_stage;
   const int* pml_off;    // [nbatch] 1 once the STA/LTA trigger switched the NPML off
-  int* flag;             // error bits: 1 non-finite trace (record kernel), 2 tensor-core wait timed out
+  int* flag;             // error bits: 1 non-finite trace (record kernel), 2 tensor-core wait timed out,
+                         // 4 halo arrival wait ran out, 8 bulk-copy wait timed out
   const float* ghost;    // learned boundary: [nbatch][nbf][9][NpF] exterior states (face code -3 - index)
   int nbf;
 };

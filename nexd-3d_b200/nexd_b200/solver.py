@@ -104,10 +104,10 @@ class Solver:
             raise _gpu_error(self._ctx, st)
 
     def set_contraction_kinds(self, npml, rest):
-        """Pins the kernel per element class ("fp32", "bf16x3"; "fp32_split"
+        """Pins the kernel per element class ("fp32", "bf16x3"; "fp32_bulk"
         for the NPML elements, "fp32_pairs" for the rest), e.g. an earlier
         auto choice, without timing."""
-        m = {"fp32": 0, "bf16x3": 1, "fp32_pairs": 2, "fp32_split": 3}
+        m = {"fp32": 0, "bf16x3": 1, "fp32_pairs": 2, "fp32_bulk": 3}
         kinds = (C.c_int32 * 2)(m.get(npml, npml), m.get(rest, rest))
         st = _abi.gpu_lib().nexd_set_contraction_kinds(self._ctx, kinds)
         if st != 0:
@@ -120,7 +120,7 @@ class Solver:
         st = _abi.gpu_lib().nexd_get_contraction(self._ctx, kinds, ms)
         if st != 0:
             raise _gpu_error(self._ctx, st)
-        names = {0: "fp32", 1: "bf16x3", 2: "fp32_pairs", 3: "fp32_split"}
+        names = {0: "fp32", 1: "bf16x3", 2: "fp32_pairs", 3: "fp32_bulk"}
         return ({"npml": names[kinds[0]], "rest": names[kinds[1]]},
                 {(cl, names[k]): ms[4 * i + k] for i, cl in enumerate(("npml", "rest")) for k in range(4)})
 

@@ -5,7 +5,8 @@ elastic cube, N=3) over all 1,000 steps and the two-layer anelastic + NPML
 family (3,000 tets, N=4, moment tensor) over all 3,000 steps -- against the
 FP64 oracle's traces stored in tests/golden/fullrun_*.npz (made by
 tests/golden/make_fullrun_fixtures.py).  Every element contraction is run: the
-FP32 CUDA-core kernels, the node-pair FP32 kernel, the split-BF16 tcgen05
+FP32 CUDA-core kernels, the node-pair FP32 kernel, the NPML kernel with
+bulk-copied element-local state, the split-BF16 tcgen05
 kernel (order 4) and the autotuned choice.  Bar: relative L2 of the traces
 <= 1e-4 per trace kind (u, v, a) over all receivers and components, after the
 full run; the misfit at intermediate steps is recorded to show how the error
@@ -25,7 +26,7 @@ import make_fullrun_fixtures as fx  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 CASES = [("cube", "fp32"), ("cube", "fp32_pairs"), ("cube", "auto"),
-         ("twolayer", "fp32"), ("twolayer", "bf16x3"), ("twolayer", "auto")]
+         ("twolayer", "fp32"), ("twolayer", "fp32_bulk"), ("twolayer", "bf16x3"), ("twolayer", "auto")]
 
 
 def _fixture(name):
@@ -40,7 +41,10 @@ def test_full_run_traces_match_fp64_oracle(tmp_path, name, contraction):
     # the rebuilt descriptor is the one the fixture was made from
     assert np.allclose(fx.fingerprint(m), ref["fingerprint"], rtol=1e-12, atol=0)
     s = Solver(m.desc_ptr)
-    s.set_contraction(contraction)
+    if contraction == "fp32_bulk":  # the NPML kernel with bulk-copied element-local state
+        s.set_contraction_kinds("fp32_bulk", "fp32")
+    else:
+        s.set_contraction(contraction)
     nt = m.nt
     growth = {}
     for lo, hi in ((1, nt // 4), (nt // 4 + 1, nt // 2), (nt // 2 + 1, nt)):
