@@ -362,6 +362,10 @@ KernelFn pick_bulk_kernel(int N, bool att, int mode, size_t& smem) {
 // Threads per block of a kernel kind.
 int kind_threads(int) { return 256; }
 
+// Floats per element of an element-blocked array of F fields: F x Np
+// padded to a multiple of 4 (EBlock in stage_kernel.cuh).
+long long block_stride(int F, int Np) { return ((long long)F * Np + 3) / 4 * 4; }
+
 int elements_per_chunk(int N) {
   const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
   return 256 / Np;
@@ -748,9 +752,14 @@ int create_impl(const nexd_desc* d, const nexd_halo_desc* h, nexd_ctx** out) {
 
   // ---- device memory ----
   const long long nodes = (long long)(K + c->nhalo) * Np;
-  c->ldq = (nodes + 63) / 64 * 64;
-  c->ldt = c->ldq;
-  c->lda = ((long long)c->Kpml * Np + 63) / 64 * 64;
+  // per-field lengths: q field-major over own and halo nodes; the
+  // element-blocked arrays (residual of q, memory variables, NPML
+  // auxiliaries) hold each element's F x Np floats padded to a multiple of 4
+  // (eblock in stage_kernel.cuh), so F ld >= elements x that
+  auto ld_blocked = [&](long long nel, int F) { return F > 0 ? (nel * block_stride(F, Np) + F - 1) / F : 0LL; };
+  c->ldq = (std::max(nodes, ld_blocked(K, 9)) + 63) / 64 * 64;
+  c->ldt = (ld_blocked(K, 6 * c->nMB) + 63) / 64 * 64;
+  c->lda = (ld_blocked(c->Kpml, 27) + 63) / 64 * 64;
   const int nb = c->nbatch;
   if ((st = upload(c, &c->D, h_D)) || (st = upload(c, &c->L, h_L)) || (st = upload(c, &c->geo, h_geo)) ||
       (st = upload(c, &c->patterns, pat)))
@@ -2697,8 +2706,9 @@ int nexd_get_traces(nexd_ctx* c, float* out) {
 namespace {
 // Device layout of a state array: (pointer to batch member b, fields, field
 // stride, elements covered).  q is field-major ([field][ld]); the memory
-// variables and NPML auxiliaries are element-blocked ([element][field][Np]
-// within the batch member's nf * ld floats).
+// variables and NPML auxiliaries are element-blocked ([element][field][Np],
+// each element's nf x Np floats padded to a multiple of 4, within the batch
+// member's nf * ld floats).
 int state_view(nexd_ctx* c, int32_t which, int32_t b, float** base, int* nf, long long* ld, int* nel) {
   if (b < 0 || b >= c->nbatch) return set_err(c, NEXD_ERR_INVALID, "batch index out of range");
   if (which == NEXD_STATE_Q) {
@@ -2735,7 +2745,7 @@ int nexd_get_state(nexd_ctx* c, int32_t which, int32_t b, float* out) {
   for (int f = 0; f < nf; ++f)
     for (int ni = 0; ni < nel; ++ni) {
       const int e = c->new2old[ni];
-      const size_t dev = blocked ? (size_t(ni) * nf + f) * c->Np : f * ld + size_t(ni) * c->Np;
+      const size_t dev = blocked ? size_t(ni) * block_stride(nf, c->Np) + size_t(f) * c->Np : f * ld + size_t(ni) * c->Np;
       std::memcpy(out + f * nodes + size_t(e) * c->Np, h.data() + dev, c->Np * sizeof(float));
     }
   return NEXD_OK;
@@ -2758,7 +2768,7 @@ int nexd_set_state(nexd_ctx* c, int32_t which, int32_t b, const float* in) {
   for (int f = 0; f < nf; ++f)
     for (int ni = 0; ni < nel; ++ni) {
       const int e = c->new2old[ni];
-      const size_t dev = blocked ? (size_t(ni) * nf + f) * c->Np : f * ld + size_t(ni) * c->Np;
+      const size_t dev = blocked ? size_t(ni) * block_stride(nf, c->Np) + size_t(f) * c->Np : f * ld + size_t(ni) * c->Np;
       std::memcpy(h.data() + dev, in + f * nodes + size_t(e) * c->Np, c->Np * sizeof(float));
     }
   CUDA_TRY(c, cudaMemcpyAsync(base, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));

@@ -371,12 +371,18 @@ constexpr int kNMB = 3;
 // Element-local state (LSERK residual of q, memory variables and their
 // residuals, NPML auxiliaries and their residuals) is element-blocked: field f
 // of node n of element e of batch member b sits at
-//   b F ld + (e F + f) Np + n,
-// so every field of a node is a compile-time offset from one address (ld >=
-// elements x Np is the per-field length, the batch stride F ld as for q).
+//   b F ld + e FS + f Np + n,   FS = F Np rounded up to a multiple of 4,
+// so every field of a node is a compile-time offset from one address, and
+// every element's block starts on a 16-byte boundary (so a chunk's block
+// range can be moved by 1-D bulk copies).  ld is the per-field length (F ld
+// >= elements x FS), F ld the batch stride.
+template <int F, int Np>
+struct EBlock {
+  static constexpr int FS = (F * Np + 3) / 4 * 4;
+};
 template <int F, int Np>
 __device__ __forceinline__ long long eblock(long long ld, int b, int e, int n) {
-  return (long long)b * F * ld + (long long)e * F * Np + n;
+  return (long long)b * F * ld + (long long)e * EBlock<F, Np>::FS + n;
 }
 
 // Update-phase state of one node, loaded into registers when the chunk starts

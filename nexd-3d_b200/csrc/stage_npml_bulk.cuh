@@ -1,34 +1,37 @@
-// NPML stage kernel with the element-local state staged by bulk copies (sm_100a, FP32).
+// NPML stage kernel with the element-local state moved by bulk copies (sm_100a, FP32).
 //
 // The same stage as stage_kernel<N, ATT, true, MODE> (the reference's element
 // loop for PML elements, src/timeloopMod.f90:395-476 with 399-405, and the
 // stage update of RungeKuttaSteps, src/rungekuttaMod.f90:27-88), with the
 // same thread-per-node mapping and the same operations in the same order, so
 // both kernels give identical results.  What changes is how a chunk's
-// element-local state reaches the threads.  stage_kernel loads it into
-// registers at the start of each chunk (63 NPML values and 45 update values
-// per node); those ~100 loads per thread are issued in one burst that the
-// memory system accepts only as fast as earlier loads return, and the block
-// (one per SM at this size) computes nothing meanwhile.  Here one thread
-// moves each array's chunk range -- element-blocked, so one contiguous range
-// per array -- with a 1-D bulk copy (cp.async.bulk, completion counted on an
-// mbarrier, no multicast) into shared memory while the block computes:
+// element-local state reaches the threads and goes back.  stage_kernel loads
+// it into registers at the start of each chunk (63 NPML values and 45 update
+// values per node) and stores the new values from registers (108 per node);
+// the memory system takes those ~200 instructions per thread in bursts only
+// as fast as earlier ones complete, and the block (one per SM at this size)
+// computes nothing meanwhile.  Here each array's chunk range -- element-
+// blocked, each element's block 16-byte aligned (eblock), so one contiguous
+// range per array -- moves between global and shared memory as one 1-D bulk
+// copy issued by one thread (cp.async.bulk; loads complete on an mbarrier,
+// stores in bulk groups; no multicast), while the block computes; the
+// threads update the state in place in shared memory:
 //
-//   buffer A   F', G', H', their residuals and the 9 damping profiles of the
-//              chunk (read in the NPML phase); refilled with the next
-//              chunk's as soon as the NPML phase has read it, so the copy
-//              overlaps the volume, lift and update phases
-//   buffer B   the LSERK residual of q, the memory variables and their
-//              residuals (read in the update phase); refilled at the start
-//              of each chunk, so the copy overlaps the face, NPML, volume
-//              and lift phases
+//   buffer A   F', G', H', their residuals (TVD: step-start values) and the
+//              9 damping profiles of the chunk, used in the NPML phase;
+//              stored back right after that phase, refilled with the next
+//              chunk's after the volume loop
+//   buffer B   the LSERK residual of q (TVD: the step-start q, read only),
+//              the memory variables and their residuals, used in the update
+//              phase; stored back at the start of the next chunk, refilled
+//              with that chunk's after its face phase
 //
-// Each range is widened to 16-byte boundaries (bulk copies move 16-byte
-// multiples between 16-byte-aligned addresses); the arrays carry 4 floats of
-// slack after their last element so the widened end stays inside them.  The
-// waits on the mbarriers are bounded: after ~2^22 polls the kernel sets
-// error bit 8 and leaves its chunk loop (every thread sees the same
-// mbarrier), and the host reports NEXD_ERR_CUDA.
+// The profiles and the TVD step-start q keep their unpadded layouts: their
+// ranges are widened to 16-byte boundaries for the loads (the arrays carry 4
+// floats of slack after the last element) and never stored.  The new q is
+// written with ordinary coalesced stores (field-major).  Waits on the
+// mbarriers are bounded: after ~2^22 polls the kernel sets error bit 8 and
+// the host reports NEXD_ERR_CUDA.
 #pragma once
 #include "stage_kernel.cuh"
 #include "tc_gemm.cuh"
@@ -40,11 +43,14 @@ struct BulkOrder {
   using O = Order<N>;
   static constexpr int Np = O::Np, E = O::E;
   static constexpr int w16(int x) { return O::r4(x + 6); }  // a range widened to 16-byte boundaries
-  static constexpr int SAUX = w16(E * 27 * Np);             // F', G', H' (and their residuals)
+  static constexpr int FA = EBlock<27, Np>::FS;             // floats per element: F', G', H'
+  static constexpr int FR = EBlock<9, Np>::FS;              // residual of q
+  static constexpr int FT = EBlock<6 * kNMB, Np>::FS;       // memory variables
+  static constexpr int SAUX = E * FA;                       // F', G', H' (and their residuals)
   static constexpr int SPRF = w16(E * 9 * Np);              // damping profiles
   static constexpr int QR = w16(E * Np);                    // one field's row of the TVD step-start q
-  static constexpr int SRES = (w16(E * 9 * Np) > 9 * QR) ? w16(E * 9 * Np) : 9 * QR;  // LSERK residual or TVD q
-  static constexpr int STH = w16(E * 6 * kNMB * Np);        // memory variables (and their residuals)
+  static constexpr int SRES = (E * FR > 9 * QR) ? E * FR : 9 * QR;  // LSERK residual or TVD step-start q
+  static constexpr int STH = E * FT;                        // memory variables (and their residuals)
   static constexpr int SA = 2 * SAUX + SPRF;
   static constexpr int SB = SRES + 2 * STH;
   // floats before the two mbarriers (8-byte aligned)
@@ -62,11 +68,22 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                "l"(src), "r"(bytes), "r"(mbar)
                : "memory");
 }
+// 1-D bulk copy shared -> global, tracked by bulk groups.
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(tc::smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until the shared memory of every committed bulk store has been read.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Waits until every committed bulk store has completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-// One array's chunk range [base, base + cnt) floats widened to 16-byte
-// boundaries: returns the bytes and starts the copy into dst; the value at
-// base + x lands at dst[(base & 3) + x].
+// One unpadded array's chunk range [base, base + cnt) floats widened to
+// 16-byte boundaries, copied into dst (the value at base + x lands at
+// dst[(base & 3) + x]); returns the bytes.
 __device__ __forceinline__ uint32_t bulk_range(float* dst, const float* arr, long long base, long long cnt,
                                                uint32_t mbar) {
   const long long s0 = base & ~3LL;
@@ -79,65 +96,95 @@ __device__ __forceinline__ uint32_t bulk_bytes(long long base, long long cnt) {
   return uint32_t((((base + cnt + 3) & ~3LL) - (base & ~3LL)) * 4);
 }
 
-// Buffer A of chunk c (one thread): F', G', H' [, residuals], profiles.
+// First float of chunk c's range in an element-blocked array of F fields.
+template <int F, int Np>
+__device__ __forceinline__ long long eblock_chunk(long long ld, const Chunk& c) {
+  return eblock<F, Np>(ld, c.b, c.e0, 0);
+}
+
+// Buffer A of chunk c (one thread): F', G', H', their residuals, profiles.
 template <int N>
-__device__ __forceinline__ void issue_state_a(const StageArgs& a, const Chunk& c, float* sAux, float* sAux2,
-                                              float* sPrf, bool need2, uint32_t mbar) {
-  constexpr int Np = Order<N>::Np;
-  const long long ba = (long long)c.b * 27 * a.lda + (long long)c.e0 * 27 * Np, na = (long long)c.ne * 27 * Np;
+__device__ __forceinline__ void load_state_a(const StageArgs& a, const Chunk& c, float* sAux, float* sAux2,
+                                             float* sPrf, uint32_t mbar) {
+  using B = BulkOrder<N>;
+  constexpr int Np = B::Np;
+  const long long ba = eblock_chunk<27, Np>(a.lda, c);
+  const uint32_t na = uint32_t(c.ne) * B::FA * 4;
   const long long bp = (long long)c.e0 * 9 * Np, np_ = (long long)c.ne * 9 * Np;
-  uint32_t bytes = bulk_bytes(ba, na) * (need2 ? 2 : 1) + bulk_bytes(bp, np_);
-  mbar_expect_tx(mbar, bytes);
-  bulk_range(sAux, a.aux, ba, na, mbar);
-  if (need2) bulk_range(sAux2, a.aux2, ba, na, mbar);
+  mbar_expect_tx(mbar, 2 * na + bulk_bytes(bp, np_));
+  bulk_load(sAux, a.aux + ba, na, mbar);
+  bulk_load(sAux2, a.aux2 + ba, na, mbar);
   bulk_range(sPrf, a.prof, bp, np_, mbar);
+}
+template <int N>
+__device__ __forceinline__ void store_state_a(const StageArgs& a, const Chunk& c, const float* sAux,
+                                              const float* sAux2) {
+  using B = BulkOrder<N>;
+  const long long ba = eblock_chunk<27, B::Np>(a.lda, c);
+  const uint32_t na = uint32_t(c.ne) * B::FA * 4;
+  bulk_store(a.aux + ba, sAux, na);
+  bulk_store(a.aux2 + ba, sAux2, na);
+  bulk_commit();
 }
 
 // Buffer B of chunk c (one thread): residual of q (LSERK) or step-start q
-// rows (TVD, field-major: one range per field), memory variables [, residuals].
+// rows (TVD, field-major: one widened range per field), memory variables and
+// their residuals.
 template <int N, bool ATT, int MODE>
-__device__ __forceinline__ void issue_state_b(const StageArgs& a, const Chunk& c, float* sRes, float* sTh,
-                                              float* sTh2, bool need2, uint32_t mbar) {
-  constexpr int Np = Order<N>::Np, E = Order<N>::E;
-  uint32_t bytes = 0;
+__device__ __forceinline__ void load_state_b(const StageArgs& a, const Chunk& c, float* sRes, float* sTh,
+                                             float* sTh2, uint32_t mbar) {
+  using B = BulkOrder<N>;
+  constexpr int Np = B::Np;
   const bool resv = (MODE == MODE_LSERK) || a.ca != 0.f;
-  const long long br = (long long)c.b * 9 * a.ldq + (long long)c.e0 * 9 * Np, nr = (long long)c.ne * 9 * Np;
+  const long long br = eblock_chunk<9, Np>(a.ldq, c);
+  const uint32_t nr = uint32_t(c.ne) * B::FR * 4;
   const long long bq = (long long)c.b * 9 * a.ldq + (long long)c.e0 * Np, nq = (long long)c.ne * Np;
-  const long long bt = (long long)c.b * 6 * kNMB * a.ldt + (long long)c.e0 * 6 * kNMB * Np,
-                  nth = (long long)c.ne * 6 * kNMB * Np;
+  const long long bt = eblock_chunk<6 * kNMB, Np>(a.ldt, c);
+  const uint32_t nt = uint32_t(c.ne) * B::FT * 4;
+  uint32_t bytes = 0;
   if (resv) {
-    if (MODE == MODE_LSERK) bytes += bulk_bytes(br, nr);
+    if (MODE == MODE_LSERK) bytes += nr;
     else
       for (int f = 0; f < 9; ++f) bytes += bulk_bytes(bq + f * a.ldq, nq);
   }
-  if (ATT) bytes += bulk_bytes(bt, nth) * (need2 ? 2 : 1);
+  if (ATT) bytes += 2 * nt;
   mbar_expect_tx(mbar, bytes);
   if (resv) {
     if (MODE == MODE_LSERK) {
-      bulk_range(sRes, a.res, br, nr, mbar);
+      bulk_load(sRes, a.res + br, nr, mbar);
     } else {
-      // TVD: step-start q, field-major; field f of the chunk at sRes[f * QR]
-      for (int f = 0; f < 9; ++f) bulk_range(sRes + f * BulkOrder<N>::QR, a.q_n, bq + f * a.ldq, nq, mbar);
+      for (int f = 0; f < 9; ++f) bulk_range(sRes + f * B::QR, a.q_n, bq + f * a.ldq, nq, mbar);
     }
   }
   if (ATT) {
-    bulk_range(sTh, a.th, bt, nth, mbar);
-    if (need2) bulk_range(sTh2, a.th2, bt, nth, mbar);
+    bulk_load(sTh, a.th + bt, nt, mbar);
+    bulk_load(sTh2, a.th2 + bt, nt, mbar);
   }
 }
+template <int N, bool ATT, int MODE>
+__device__ __forceinline__ void store_state_b(const StageArgs& a, const Chunk& c, const float* sRes, const float* sTh,
+                                              const float* sTh2) {
+  using B = BulkOrder<N>;
+  constexpr int Np = B::Np;
+  if (MODE == MODE_LSERK) bulk_store(a.res + eblock_chunk<9, Np>(a.ldq, c), sRes, uint32_t(c.ne) * B::FR * 4);
+  if (ATT) {
+    const long long bt = eblock_chunk<6 * kNMB, Np>(a.ldt, c);
+    bulk_store(a.th + bt, sTh, uint32_t(c.ne) * B::FT * 4);
+    bulk_store(a.th2 + bt, sTh2, uint32_t(c.ne) * B::FT * 4);
+  }
+  bulk_commit();
+}
 
-// pml_update with the node's damping profiles, auxiliaries and their
-// residuals (TVD: step-start values) read from shared memory at a stride of
-// Np floats; the same operations in the same order.
+// pml_update with the node's damping profiles pr, auxiliaries av and their
+// residuals a2 (TVD: step-start values) in shared memory at a stride of Np
+// floats, updated there in place; the same operations in the same order.
 template <int Np, int MODE>
-__device__ __forceinline__ void pml_update_strided(const StageArgs& a, int b, int e, int n, bool off, const float* pr,
-                                                   const float* av, const float* a2, float* F, float* G, float* H) {
+__device__ __forceinline__ void pml_update_smem(const StageArgs& a, bool off, const float* pr, float* av, float* a2,
+                                                float* F, float* G, float* H) {
   if (off) return;  // pmlcheck(:) = .false.: ordinary element (src/timeloopMod.f90:537)
   const float ddx = pr[0], ddy = pr[Np], ddz = pr[2 * Np];
   const float alx = pr[3 * Np], aly = pr[4 * Np], alz = pr[5 * Np];
   const float ikx = 1.f / pr[6 * Np], iky = 1.f / pr[7 * Np], ikz = 1.f / pr[8 * Np];
-  float* aux = a.aux + eblock<27, Np>(a.lda, b, e, n);
-  float* aux2 = a.aux2 + eblock<27, Np>(a.lda, b, e, n);
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     const float fp = av[i * Np], gp = av[(9 + i) * Np], hp = av[(18 + i) * Np];
@@ -150,18 +197,18 @@ __device__ __forceinline__ void pml_update_strided(const StageArgs& a, int b, in
       const float r1 = a.ca * a2[i * Np] + a.dt * rf;
       const float r2 = a.ca * a2[(9 + i) * Np] + a.dt * rg;
       const float r3 = a.ca * a2[(18 + i) * Np] + a.dt * rh;
-      __stcs(aux2 + i * Np, r1);
-      __stcs(aux2 + (9 + i) * Np, r2);
-      __stcs(aux2 + (18 + i) * Np, r3);
+      a2[i * Np] = r1;
+      a2[(9 + i) * Np] = r2;
+      a2[(18 + i) * Np] = r3;
       nf = fp + a.cb * r1;
       ng_ = gp + a.cb * r2;
       nh = hp + a.cb * r3;
     } else {
       float n1, n2, n3;
       if (a.stage_first) {
-        __stcs(aux2 + i * Np, fp);
-        __stcs(aux2 + (9 + i) * Np, gp);
-        __stcs(aux2 + (18 + i) * Np, hp);
+        a2[i * Np] = fp;
+        a2[(9 + i) * Np] = gp;
+        a2[(18 + i) * Np] = hp;
         n1 = fp; n2 = gp; n3 = hp;
       } else {
         n1 = a2[i * Np]; n2 = a2[(9 + i) * Np]; n3 = a2[(18 + i) * Np];
@@ -170,26 +217,25 @@ __device__ __forceinline__ void pml_update_strided(const StageArgs& a, int b, in
       ng_ = a.ca * n2 + a.cb * (gp + a.dt * rg);
       nh = a.ca * n3 + a.cb * (hp + a.dt * rh);
     }
-    __stcs(aux + i * Np, nf);
-    __stcs(aux + (9 + i) * Np, ng_);
-    __stcs(aux + (18 + i) * Np, nh);
+    av[i * Np] = nf;
+    av[(9 + i) * Np] = ng_;
+    av[(18 + i) * Np] = nh;
     F[i] = phi;
     G[i] = psi;
     H[i] = ome;
   }
 }
 
-// finish_node with the node's update-phase state read from shared memory:
-// rs[c * rstride] the residual of q (TVD: step-start q), th / th2 the memory
-// variables and their residuals (TVD: step-start values) at a stride of Np.
+// finish_node with the node's update-phase state in shared memory, updated
+// there in place: rs[c * rstride] the residual of q (TVD: step-start q, read
+// only), th / th2 the memory variables and their residuals (TVD: step-start
+// values) at a stride of Np.  The new q goes to global memory.
 template <int Np, bool ATT, int MODE>
-__device__ __forceinline__ void finish_node_strided(const StageArgs& a, int b, int e, long long node, float* rq,
-                                                    const float* S, const float* rs, int rstride, const float* ths,
-                                                    const float* th2s, const float* qown, int qstride, bool need2) {
+__device__ __forceinline__ void finish_node_smem(const StageArgs& a, int b, int e, long long node, float* rq,
+                                                 const float* S, float* rs, int rstride, float* ths, float* th2s,
+                                                 const float* qown, int qstride) {
   const int n = int(node - (long long)e * Np);
   if (ATT) {
-    float* th = a.th + eblock<6 * kNMB, Np>(a.ldt, b, e, n);
-    float* th2 = a.th2 + eblock<6 * kNMB, Np>(a.ldt, b, e, n);
     const float* ae = a.ael + (long long)e * 3 * kNMB;
 #pragma unroll
     for (int l = 0; l < kNMB; ++l) {
@@ -198,7 +244,7 @@ __device__ __forceinline__ void finish_node_strided(const StageArgs& a, int b, i
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
         t[j] = ths[(6 * l + j) * Np];
-        t2[j] = need2 ? th2s[(6 * l + j) * Np] : 0.f;
+        t2[j] = th2s[(6 * l + j) * Np];
       }
       const float c1 = ae[3 * l], c2 = ae[3 * l + 1], c3 = ae[3 * l + 2];
       rq[0] += c3 * t[0] + c1 * (t[1] + t[2]);
@@ -214,14 +260,14 @@ __device__ __forceinline__ void finish_node_strided(const StageArgs& a, int b, i
         float nt_;
         if (MODE == MODE_LSERK) {
           const float rr = a.ca * t2[j] + a.dt * r;
-          __stcs(th2 + o, rr);
+          th2s[o] = rr;
           nt_ = t[j] + a.cb * rr;
         } else {
           float tn;
-          if (a.stage_first) { __stcs(th2 + o, t[j]); tn = t[j]; } else { tn = t2[j]; }
+          if (a.stage_first) { th2s[o] = t[j]; tn = t[j]; } else { tn = t2[j]; }
           nt_ = a.ca * tn + a.cb * (t[j] + a.dt * r);
         }
-        __stcs(th + o, nt_);
+        ths[o] = nt_;
       }
     }
   }
@@ -244,11 +290,10 @@ __device__ __forceinline__ void finish_node_strided(const StageArgs& a, int b, i
   }
   float* qo = a.q_out + (long long)b * 9 * a.ldq + node;
   if (MODE == MODE_LSERK) {
-    float* rsg = a.res + eblock<9, Np>(a.ldq, b, e, n);
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
       const float r = a.ca * rs[c * rstride] + a.dt * rq[c];
-      __stcs(rsg + c * Np, r);
+      rs[c * rstride] = r;
       __stcs(qo + c * a.ldq, qown[c * qstride] + a.cb * r);
     }
   } else {
@@ -309,7 +354,6 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
     le = tid / Np;
     n = tid - le * Np;
   }
-  const bool need2 = (MODE == MODE_LSERK) || !a.stage_first;
   int w = blockIdx.x;
   if (w >= nwork) return;
 
@@ -331,30 +375,31 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
     }
     __syncthreads();
     if (tid == 0) {
-      issue_state_a<N>(a, c0, sAux, sAux2, sPrf, need2, mbarA);
-      issue_state_b<N, ATT, MODE>(a, c0, sRes, sTh, sTh2, need2, mbarB);
+      load_state_a<N>(a, c0, sAux, sAux2, sPrf, mbarA);
+      load_state_b<N, ATT, MODE>(a, c0, sRes, sTh, sTh2, mbarB);
     }
     issue_chunk<O>(a, c0, ids0, sBuf, wn < nwork ? &c1 : nullptr, sPat);
   }
 
+  bool ok = true;
   uint32_t phase = 0;  // parity of both mbarriers' current phase (each completes once per chunk)
+  Chunk prev;
   for (int p = 0; w < nwork; w += gridDim.x, p ^= 1, phase ^= 1) {
     const Chunk ch = chunk_of<E>(a, w, nchunk);
     const int b = ch.b, e0 = ch.e0, ne = ch.ne;
+    const bool first = w == (int)blockIdx.x;
     float* buf = sBuf + p * O::BUF;
     const float* sGeo = buf;
     const float* sTr = buf + O::SGEO + O::SQF;
     const float* sQF = buf + O::SGEO + int(((long long)e0 * Np) & 3);
     const int* sIds = reinterpret_cast<const int*>(sTr + O::STR);
     cp_async_wait_all();
-    __syncthreads();  // (1) this chunk's records, wavefield and traces are in `buf`; buffer B is free
+    __syncthreads();  // (1) records, wavefield and traces in `buf`; the previous chunk's buffer B is final
+    // the previous chunk's residual and memory variables go back to global memory
+    if (tid == 0 && !first) store_state_b<N, ATT, MODE>(a, prev, sRes, sTh, sTh2);
     const int wn = w + gridDim.x;
     Chunk cn;
     if (wn < nwork) cn = chunk_of<E>(a, wn, nchunk);
-    if (tid == 0 && w != (int)blockIdx.x) {
-      tc::fence_async_smem();
-      issue_state_b<N, ATT, MODE>(a, ch, sRes, sTh, sTh2, need2, mbarB);
-    }
     const bool active = le < ne;
     const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
     if (wn < nwork) {
@@ -381,18 +426,22 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
       am[O::NFP] = as1 * fs;
       am[2 * O::NFP] = as2 * fs;
     }
-    // ---- NPML: auxiliary update and contravariant modified fluxes ------------------
+    // buffer B was read by its store long ago: refill it with this chunk's state
+    if (tid == 0 && !first) {
+      bulk_wait_read();
+      load_state_b<N, ATT, MODE>(a, ch, sRes, sTh, sTh2, mbarB);
+    }
+    // ---- NPML: auxiliary update (in place) and contravariant modified fluxes -------
     const bool okA = tc::mbar_wait(mbarA, phase);
-    if (active) {
+    if (active && okA) {
       const float* g = sGeo + le * O::GSTR;
       float qv[9];
 #pragma unroll
       for (int c = 0; c < 9; ++c) qv[c] = sQF[c * O::QF + le * Np + n];
       float F[9], G[9], H[9];
       elastic_fluxes(g, qv, F, G, H);
-      const int so = int(((long long)b * 27 * a.lda + (long long)e0 * 27 * Np) & 3) + le * 27 * Np + n;
       const float* ps = sPrf + int(((long long)e0 * 9 * Np) & 3) + le * 9 * Np + n;
-      pml_update_strided<Np, MODE>(a, b, e0 + le, n, a.pml_off[b] != 0, ps, sAux + so, sAux2 + so, F, G, H);
+      pml_update_smem<Np, MODE>(a, a.pml_off[b] != 0, ps, sAux + le * B::FA + n, sAux2 + le * B::FA + n, F, G, H);
       float2* cf = reinterpret_cast<float2*>(sCF + le * O::CFE + n * CS);
       float r[10], sv[10], t[10];
 #pragma unroll
@@ -411,17 +460,15 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
         cf[10 + j] = make_float2(t[2 * j], t[2 * j + 1]);
       }
     }
-    if (__syncthreads_or(!okA)) {  // (2) amplitudes and rows are in shared memory; buffer A is consumed
-      if (tid == 0) atomicOr(a.flag, 8);
+    tc::fence_async_smem();  // this thread's writes to buffer A are seen by the bulk store
+    if (__syncthreads_or(!okA)) {  // (2) amplitudes and rows are in shared memory; buffer A is final
+      ok = false;
       break;
     }
-    if (tid == 0 && wn < nwork) {
-      tc::fence_async_smem();
-      issue_state_a<N>(a, cn, sAux, sAux2, sPrf, need2, mbarA);
-    }
+    if (tid == 0) store_state_a<N>(a, ch, sAux, sAux2);
     if (!active) {
-      // idle threads of a partial chunk still take part in the update-phase wait below
-      if (!tc::mbar_wait(mbarB, phase)) atomicOr(a.flag, 8);
+      // idle threads of a partial chunk: thread 0 is never idle, so nothing else to do
+      prev = ch;
       continue;
     }
 
@@ -474,6 +521,11 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
         }
       }
     }
+    // buffer A was read by its store during the volume loop: refill it with the next chunk's
+    if (tid == 0 && wn < nwork) {
+      bulk_wait_read();
+      load_state_a<N>(a, cn, sAux, sAux2, sPrf, mbarA);
+    }
     float sig_an[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) sig_an[c] = 0.f;
@@ -508,25 +560,37 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
       S[4] = sig_an[4] - 0.5f * (vgrad[7] + vgrad[5]);
       S[5] = sig_an[5] - 0.5f * (vgrad[6] + vgrad[2]);
     }
-    // ---- memory variables, sources, receivers, stage update (state from buffer B)
-    if (!tc::mbar_wait(mbarB, phase)) {
-      atomicOr(a.flag, 8);
-      continue;  // the next top-of-chunk barrier is reached by every thread
-    }
-    {
-      const float* rs;
+    // ---- memory variables, sources, receivers, stage update (state in buffer B) ---
+    if (tc::mbar_wait(mbarB, phase)) {
+      float* rs;
       int rstride;
       if (MODE == MODE_LSERK) {
-        rs = sRes + int(((long long)b * 9 * a.ldq + (long long)e0 * 9 * Np) & 3) + le * 9 * Np + n;
+        rs = sRes + le * B::FR + n;
         rstride = Np;
       } else {
         rs = sRes + int(((long long)b * 9 * a.ldq + (long long)e0 * Np) & 3) + le * Np + n;
         rstride = B::QR;
       }
-      const int to = int(((long long)b * 6 * kNMB * a.ldt + (long long)e0 * 6 * kNMB * Np) & 3) + le * 6 * kNMB * Np + n;
-      finish_node_strided<Np, ATT, MODE>(a, b, e, node, rq, S, rs, rstride, sTh + to, sTh2 + to,
-                                         sQF + le * Np + n, O::QF, need2);
+      finish_node_smem<Np, ATT, MODE>(a, b, e, node, rq, S, rs, rstride, sTh + le * B::FT + n,
+                                      sTh2 + le * B::FT + n, sQF + le * Np + n, O::QF);
+    } else {
+      atomicOr(a.flag, 8);
     }
+    tc::fence_async_smem();  // this thread's writes to buffer B are seen by the bulk store
+    prev = ch;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (ok) {
+      store_state_b<N, ATT, MODE>(a, prev, sRes, sTh, sTh2);
+    } else {
+      // a load did not complete in time: wait once more, again bounded, for
+      // the loads of this chunk still in flight before the block exits
+      atomicOr(a.flag, 8);
+      tc::mbar_wait(mbarA, phase, 1u << 24);
+      tc::mbar_wait(mbarB, phase, 1u << 24);
+    }
+    bulk_wait_all();
   }
   cp_async_wait_all();
 }
