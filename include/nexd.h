@@ -273,16 +273,17 @@ int nexd_set_contraction(nexd_ctx* ctx, int32_t mode);
 
 /* The kernel kind in use per element class (kinds[0] NPML elements, kinds[1]
  * the rest: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3, 2 = the node-pair FP32
- * kernel (the rest) or 3 = the FP32 NPML kernel whose element-local state
- * arrives in shared memory by bulk copies (NPML elements)) and, after an AUTO selection, the measured ms per stage launch
+ * kernel (the rest) or 3 = the FP32 kernel whose element-local state moves
+ * between global and shared memory by bulk copies) and, after an AUTO selection, the measured ms per stage launch
  * tune_ms[class * 4 + kind] (8 floats; 0 where not measured).  Either pointer
  * may be NULL. */
 int nexd_get_contraction(const nexd_ctx* ctx, int32_t* kinds, float* tune_ms);
 
 /* Pins the kernel per element class without timing: kinds[0] for NPML
  * elements (NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3 or 3 = the bulk-copy
- * NPML kernel, orders 3 and 4), kinds[1] for the rest (the first two or 2 = the
- * node-pair FP32 kernel), as nexd_get_contraction reports them -- e.g. to replay an earlier AUTO choice, so that repeated or
+ * kernel, orders 3 and 4), kinds[1] for the rest (the first two, 2 = the
+ * node-pair FP32 kernel or 3 = the bulk-copy kernel, anelastic models,
+ * orders 2-5), as nexd_get_contraction reports them -- e.g. to replay an earlier AUTO choice, so that repeated or
  * profiled runs use the same kernels.  NEXD_ERR_UNSUPPORTED for a kind the
  * order lacks, NEXD_ERR_INVALID for an unknown kind. */
 int nexd_set_contraction_kinds(nexd_ctx* ctx, const int32_t* kinds);

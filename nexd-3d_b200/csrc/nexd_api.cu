@@ -20,7 +20,7 @@
 #include "stage_kernel.cuh"
 #include "stage_tc.cuh"
 #include "stage_pair.cuh"
-#include "stage_npml_bulk.cuh"
+#include "stage_main_bulk.cuh"
 #include "group_kernel.cuh"
 #include "boundary_mlp.cuh"
 #include "halo.cuh"
@@ -332,12 +332,13 @@ KernelFn pick_pair_kernel(int N, bool att, int mode, size_t& smem) {
 }
 
 // Kernel kinds per element class: NEXD_CONTRACT_FP32, NEXD_CONTRACT_BF16X3,
-// the node-pair FP32 kernel (elements outside the NPML) and the FP32 NPML
-// kernel whose element-local state arrives by bulk copies (NPML elements);
-// the last two give the same results as NEXD_CONTRACT_FP32 and are chosen
-// by the autotune or pinned.
+// the node-pair FP32 kernel (elements outside the NPML) and the FP32 kernels
+// whose element-local state moves by bulk copies (NPML elements: NPML and
+// update-phase state; the rest, anelastic: memory variables); the last two
+// give the same results as NEXD_CONTRACT_FP32 and are chosen by the autotune
+// or pinned.
 constexpr int KIND_FP32_PAIRS = 2;
-constexpr int KIND_NPML_BULK = 3;
+constexpr int KIND_BULK = 3;
 constexpr int NKINDS = 4;
 
 template <int N>
@@ -357,6 +358,28 @@ KernelFn pick_bulk_kernel(int N, bool att, int mode, size_t& smem) {
     case 4: smem = size_t(BulkOrder<4>::smem_floats()) * 4; return pick_bulk<4>(att, mode);
     default: smem = 0; return nullptr;
   }
+}
+
+template <int N>
+KernelFn pick_main_bulk(int mode) {
+  return mode == MODE_LSERK ? stage_main_bulk_kernel<N, MODE_LSERK> : stage_main_bulk_kernel<N, MODE_TVD>;
+}
+
+// The bulk-copy kernel for the elements outside the NPML (anelastic models,
+// orders 2-5).
+KernelFn pick_main_bulk_kernel(int N, int mode, size_t& smem) {
+  switch (N) {
+    case 2: smem = size_t(MainBulkOrder<2>::smem_floats()) * 4; return pick_main_bulk<2>(mode);
+    case 3: smem = size_t(MainBulkOrder<3>::smem_floats()) * 4; return pick_main_bulk<3>(mode);
+    case 4: smem = size_t(MainBulkOrder<4>::smem_floats()) * 4; return pick_main_bulk<4>(mode);
+    case 5: smem = size_t(MainBulkOrder<5>::smem_floats()) * 4; return pick_main_bulk<5>(mode);
+    default: smem = 0; return nullptr;
+  }
+}
+
+// Whether the bulk-copy kernel exists for an element class of this context.
+bool bulk_supported(int N, bool att, int cls) {
+  return cls == 0 ? bulk_order_supported(N) : (att && N >= 2 && N <= 5);
 }
 
 // Threads per block of a kernel kind.
@@ -506,8 +529,10 @@ int configure_launch(nexd_ctx* c) {
     } else if (c->kind[which] == KIND_FP32_PAIRS && !pmlk) {
       fn = reinterpret_cast<const void*>(pick_pair_kernel(c->N, c->att, mode, smem));
       E *= 2;
-    } else if (c->kind[which] == KIND_NPML_BULK && pmlk) {
+    } else if (c->kind[which] == KIND_BULK && pmlk) {
       fn = reinterpret_cast<const void*>(pick_bulk_kernel(c->N, c->att, mode, smem));
+    } else if (c->kind[which] == KIND_BULK && c->att) {
+      fn = reinterpret_cast<const void*>(pick_main_bulk_kernel(c->N, mode, smem));
     } else {
       fn = reinterpret_cast<const void*>(pick_kernel(c->N, c->att, pmlk, mode, smem));
     }
@@ -1047,8 +1072,11 @@ void launch_class(nexd_ctx* c, StageArgs& a, bool pml) {
   } else if (c->kind[cls] == KIND_FP32_PAIRS && !pml) {
     KernelFn f = pick_pair_kernel(c->N, c->att, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);
-  } else if (c->kind[cls] == KIND_NPML_BULK && pml) {
+  } else if (c->kind[cls] == KIND_BULK && pml) {
     KernelFn f = pick_bulk_kernel(c->N, c->att, mode, smem);
+    f<<<grid, 256, sm, c->stream>>>(a);
+  } else if (c->kind[cls] == KIND_BULK && c->att) {
+    KernelFn f = pick_main_bulk_kernel(c->N, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);
   } else {
     KernelFn f = pick_kernel(c->N, c->att, pml, mode, smem);
@@ -1521,7 +1549,8 @@ int time_class(nexd_ctx* c, bool pml, int reps, float& ms) {
 // kernel, the tensor-core kernel (order 4; FP32-accurate, agrees with the
 // FP32 kernel to FP32 rounding, not bit for bit) and the FP32 variants with
 // the same results: the node-pair kernel outside the NPML (orders 2-5), the
-// kernel with bulk-copied element-local state on NPML elements (orders 3, 4).
+// kernels with bulk-copied element-local state (NPML elements: orders 3, 4;
+// the rest: anelastic models, orders 2-5).
 int autotune(nexd_ctx* c) {
   if (int st = finish(c)) return st;  // at a step boundary
   for (int cls = 0; cls < 2; ++cls) {
@@ -1531,7 +1560,7 @@ int autotune(nexd_ctx* c) {
     for (int k = 0; k < NKINDS; ++k) {
       if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N)) continue;
       if (k == KIND_FP32_PAIRS && (cls == 0 || c->N < 2 || c->N > 5)) continue;
-      if (k == KIND_NPML_BULK && (cls == 1 || !bulk_order_supported(c->N))) continue;
+      if (k == KIND_BULK && !bulk_supported(c->N, c->att, cls)) continue;
       c->kind[cls] = k;
       if (int st = configure_launch(c)) return st;
       if (int st = time_class(c, cls == 0, 3, c->tune_ms[cls][k])) return st;
@@ -1581,10 +1610,11 @@ int nexd_set_contraction_kinds(nexd_ctx* c, const int32_t* kinds) {
   for (int cls = 0; cls < 2; ++cls) {
     const int k = kinds[cls];
     if (k != NEXD_CONTRACT_FP32 && k != NEXD_CONTRACT_BF16X3 && !(cls == 1 && k == KIND_FP32_PAIRS) &&
-        !(cls == 0 && k == KIND_NPML_BULK))
+        k != KIND_BULK)
       return set_err(c, NEXD_ERR_INVALID, "unknown kernel kind for this element class");
-    if (k == KIND_NPML_BULK && !bulk_order_supported(c->N))
-      return set_err(c, NEXD_ERR_UNSUPPORTED, "the bulk-copy NPML kernel covers orders 3 and 4");
+    if (k == KIND_BULK && !bulk_supported(c->N, c->att, cls))
+      return set_err(c, NEXD_ERR_UNSUPPORTED,
+                     "the bulk-copy kernels cover NPML elements at orders 3 and 4 and anelastic elements at orders 2-5");
     if (k == NEXD_CONTRACT_BF16X3 && !tc_order_supported(c->N))
       return set_err(c, NEXD_ERR_UNSUPPORTED, "the tensor-core contraction covers order 4");
     if (k == KIND_FP32_PAIRS && (c->N < 2 || c->N > 5))

@@ -330,14 +330,15 @@ __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, f
 
 // Asynchronous gather of the neighbour face traces of one chunk's interior
 // faces through the face patterns, using its connectivity `ids` (staged one
-// chunk earlier).  No commit.
+// chunk earlier): face nodes [lo, hi) of the chunk (hi < 0: all).  No commit.
 template <class O>
 __device__ __forceinline__ void issue_traces(const StageArgs& a, const Chunk& c, const int* ids, float* bTr,
-                                             const unsigned char* pat) {
+                                             const unsigned char* pat, int lo = 0, int hi = -1) {
   constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF;
   const int tid = threadIdx.x, nth = blockDim.x;
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
-  for (int i = tid; i < c.ne * NF; i += nth) {
+  const int end = hi < 0 ? c.ne * NF : hi;
+  for (int i = lo + tid; i < end; i += nth) {
     const int ee = i / NF, j = i - ee * NF;
     const int f = j / NpF, fi = j - f * NpF;
     const int code = ids[ee * 12 + 4 + f];
@@ -363,6 +364,26 @@ __device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, 
   issue_main<O>(a, c, bGeo, bQ, bIds, next);
   issue_traces<O>(a, c, ids, bTr, pat);
   cp_async_commit();
+}
+
+// The trace gather of a chunk split into three slices of its face nodes,
+// issued at three points of the chunk before it (each its own commit group),
+// so the gathers overlap the compute phases (used by the bulk-copy stage
+// kernels: 1.3 % shorter NPML launches than one gather burst).
+constexpr int kTraceSlices = 3;
+template <class O>
+__device__ __forceinline__ void issue_trace_slice(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
+                                                  const unsigned char* pat, int s) {
+  const int n = c.ne * O::NF;
+  issue_traces<O>(a, c, ids, buf + O::SGEO + O::SQF, pat, s * n / kTraceSlices, (s + 1) * n / kTraceSlices);
+  cp_async_commit();
+}
+// Records, wavefield and connectivity of a chunk plus its first trace slice.
+template <class O>
+__device__ __forceinline__ void issue_chunk_head(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
+                                                 const Chunk* next, const unsigned char* pat) {
+  issue_main<O>(a, c, buf, buf + O::SGEO, reinterpret_cast<int*>(buf + O::SGEO + O::SQF + O::STR), next);
+  issue_trace_slice<O>(a, c, ids, buf, pat, 0);
 }
 
 // Memory variables per mechanism set: the reference's nMB = 3 (src/constants.h:36).

@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
       const int wnn = wn + gridDim.x;
       Chunk cnn;
       if (wnn < nwork) cnn = chunk_of<E>(a, wnn, nchunk);
-      issue_chunk<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, wnn < nwork ? &cnn : nullptr, sPat);
+      issue_chunk_head<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, wnn < nwork ? &cnn : nullptr, sPat);
     }
     // ---- face amplitudes ---------------------------------------------------------
     for (int i = tid; i < ne * NF; i += blockDim.x) {
@@ -426,6 +426,7 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
       am[O::NFP] = as1 * fs;
       am[2 * O::NFP] = as2 * fs;
     }
+    if (wn < nwork) issue_trace_slice<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, sPat, 1);
     // buffer B was read by its store long ago: refill it with this chunk's state
     if (tid == 0 && !first) {
       bulk_wait_read();
@@ -466,6 +467,7 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
       break;
     }
     if (tid == 0) store_state_a<N>(a, ch, sAux, sAux2);
+    if (wn < nwork) issue_trace_slice<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, sPat, 2);
     if (!active) {
       // idle threads of a partial chunk: thread 0 is never idle, so nothing else to do
       prev = ch;

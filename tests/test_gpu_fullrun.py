@@ -41,8 +41,8 @@ def test_full_run_traces_match_fp64_oracle(tmp_path, name, contraction):
     # the rebuilt descriptor is the one the fixture was made from
     assert np.allclose(fx.fingerprint(m), ref["fingerprint"], rtol=1e-12, atol=0)
     s = Solver(m.desc_ptr)
-    if contraction == "fp32_bulk":  # the NPML kernel with bulk-copied element-local state
-        s.set_contraction_kinds("fp32_bulk", "fp32")
+    if contraction == "fp32_bulk":  # the kernels with bulk-copied element-local state
+        s.set_contraction_kinds("fp32_bulk", "fp32_bulk")
     else:
         s.set_contraction(contraction)
     nt = m.nt

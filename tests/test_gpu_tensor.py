@@ -170,9 +170,9 @@ def test_autotune_leaves_state_and_picks_valid_kinds(tmp_path, oracle, Solver, t
         assert np.array_equal(x, y)
     kinds, ms = s.contraction()
     assert set(kinds.values()) <= {"fp32", "bf16x3", "fp32_pairs", "fp32_bulk"}
-    assert kinds["npml"] != "fp32_pairs" and kinds["rest"] != "fp32_bulk"
+    assert kinds["npml"] != "fp32_pairs"
     # every candidate of each class was timed, the chosen one is the fastest
-    for cl, cands in (("npml", ("fp32", "bf16x3", "fp32_bulk")), ("rest", ("fp32", "bf16x3", "fp32_pairs"))):
+    for cl, cands in (("npml", ("fp32", "bf16x3", "fp32_bulk")), ("rest", ("fp32", "bf16x3", "fp32_pairs", "fp32_bulk"))):
         assert all(ms[(cl, k)] > 0 for k in cands)
         assert ms[(cl, kinds[cl])] == min(ms[(cl, k)] for k in cands)
     s.run(31, 60)
@@ -237,24 +237,26 @@ def test_pinned_kernel_kinds(tmp_path, oracle, Solver):
 
 
 @pytest.mark.parametrize("N,att,timeint", [(3, False, 4), (3, True, 4), (4, True, 4), (4, False, 4), (4, True, 2),
-                                          (4, True, 3)])
-def test_npml_bulk_kernel_is_bit_identical(tmp_path, oracle, Solver, N, att, timeint):
-    """The NPML kernel whose element-local state (NPML auxiliaries, their
-    residuals, damping profiles, residual of q, memory variables) arrives in
-    shared memory by bulk copies performs the FP32 NPML kernel's operations in
-    the same order: identical wavefields, memory variables, NPML auxiliaries
-    and traces under LSERK4 and the reference's RK2 and RK3, over several
-    chunks per block and partial chunks; its traces agree with the FP64
-    oracle within the FP32 tolerance; AUTO times it for the NPML class."""
+                                          (4, True, 3), (2, True, 4), (5, True, 4)])
+def test_bulk_kernels_are_bit_identical(tmp_path, oracle, Solver, N, att, timeint):
+    """The stage kernels whose element-local state moves by bulk copies (NPML
+    elements: NPML auxiliaries, their residuals, damping profiles, residual of
+    q and memory variables, orders 3 and 4; the other elements of anelastic
+    models: memory variables, orders 2-5) perform the FP32 kernels'
+    operations in the same order: identical wavefields, memory variables,
+    NPML auxiliaries and traces under LSERK4 and the reference's RK2 and RK3,
+    over several chunks per block and partial chunks; their traces agree with
+    the FP64 oracle within the FP32 tolerance; AUTO times them."""
     d = str(tmp_path / "bulk")
     nt = 40
     synth.write_twolayer(d, cells=(10, 10, 5), nt=nt, nrec=6, src_depth=(900.0, 900.0), attenuation=att)
     m = Mesh(d, N=N, stf_stage_time=(timeint == 4), timeint=timeint, cfl=0.3 if timeint == 4 else 0.1)
     assert m.array("pmlcheck").sum() > 0
+    kinds = ("fp32_bulk" if N in (3, 4) else "fp32", "fp32_bulk" if att else "fp32")
     a, b = Solver(m.desc_ptr), Solver(m.desc_ptr)
     a.set_contraction_kinds("fp32", "fp32")
-    b.set_contraction_kinds("fp32_bulk", "fp32")
-    assert b.contraction()[0] == {"npml": "fp32_bulk", "rest": "fp32"}
+    b.set_contraction_kinds(*kinds)
+    assert b.contraction()[0] == {"npml": kinds[0], "rest": kinds[1]}
     a.run(1, nt)
     b.run(1, nt)
     assert np.array_equal(a.field(), b.field())
@@ -270,18 +272,22 @@ def test_npml_bulk_kernel_is_bit_identical(tmp_path, oracle, Solver, N, att, tim
         kinds, ms = c.contraction()
         assert ms[("npml", "fp32_bulk")] > 0 and ms[("npml", "fp32")] > 0
         assert kinds["npml"] in ("fp32", "bf16x3", "fp32_bulk")
+        if att:
+            assert ms[("rest", "fp32_bulk")] > 0
 
 
-@pytest.mark.parametrize("N", [2, 5])
-def test_npml_bulk_kernel_refused_where_it_does_not_fit(tmp_path, Solver, N):
+@pytest.mark.parametrize("N,att", [(2, True), (5, True), (4, False)])
+def test_bulk_kernels_refused_where_they_do_not_apply(tmp_path, Solver, N, att):
     """Orders 2 and 5 need more shared memory than a block can have for the
-    bulk-copy NPML kernel: pinning it is refused, the FP32 kernel stays."""
+    bulk-copy NPML kernel, and elastic models have no memory variables for
+    the other bulk-copy kernel: pinning them is refused, the FP32 kernels
+    stay."""
     d = str(tmp_path / "nofit")
-    synth.write_twolayer(d, cells=(6, 6, 3), nt=4, nrec=2, src_depth=(900.0, 900.0))
+    synth.write_twolayer(d, cells=(6, 6, 3), nt=4, nrec=2, src_depth=(900.0, 900.0), attenuation=att)
     m = Mesh(d, N=N)
     s = Solver(m.desc_ptr)
     with pytest.raises(NexdError) as ei:
-        s.set_contraction_kinds("fp32_bulk", "fp32")
+        s.set_contraction_kinds("fp32_bulk", "fp32") if N != 4 else s.set_contraction_kinds("fp32", "fp32_bulk")
     assert ei.value.status == _abi.NEXD_ERR_UNSUPPORTED
     assert s.contraction()[0] == {"npml": "fp32", "rest": "fp32"}
     s.run(1, 4)
