@@ -543,7 +543,7 @@ def main():
             "metric": metric, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": dev_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32" if set(ckinds.values()) == {"fp32"} else
+            "dtype": "f32" if "bf16x3" not in ckinds.values() else
                      "f32 state and update; contraction as three-way split bf16 on tcgen05 with f32 accumulation",
             "data": "synthetic (seeded two-layer model, per-rank seeded source)",
             "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "Np": mesh.Np, "nt": mesh.nt,
