@@ -110,3 +110,33 @@ def test_partition_errors_and_bounded_wait(tmp_path, solver_mod):
     a.close()
     b.close()
     ps.close()
+
+
+def test_bulk_kernels_in_partitions_and_batches(tmp_path, solver_mod):
+    """The stage kernels whose element-local state moves by bulk copies (NPML
+    elements and the other anelastic elements), run on two wavefields per
+    launch and on partitions linked by the halo exchange, give the FP32
+    kernels' traces and wavefields on the whole mesh bit for bit."""
+    d = str(tmp_path / "tl")
+    synth.write_twolayer(d, cells=(8, 8, 4), nt=30, nrec=8, nsrc=2, src_depth=(900.0, 900.0))
+    m = Mesh(d, N=3, stf_stage_time=True, nbatch=2)
+    ref = solver_mod.Solver(m.desc_ptr)
+    ref.run(1, 20)
+    tr0, q0, q1 = ref.traces(), ref.field(0), ref.field(1)
+    ref.close()
+    s = solver_mod.Solver(m.desc_ptr)
+    s.set_contraction_kinds("fp32_bulk", "fp32_bulk")
+    s.run(1, 20)
+    assert np.array_equal(s.traces(), tr0)
+    assert np.array_equal(s.field(0), q0) and np.array_equal(s.field(1), q1)
+    s.close()
+    ps = Partitions(m.desc_ptr, 3, centroids=element_centroids(m))
+    p = PartitionedSolver(ps, nrec_total=m.nrec)
+    for sv in p.solvers:
+        sv.set_contraction_kinds("fp32_bulk", "fp32_bulk")
+    p.run(1, 9)
+    p.run(10, 20)
+    assert np.array_equal(p.traces(), tr0)
+    assert np.array_equal(p.field(m.K, m.Np, 0), q0) and np.array_equal(p.field(m.K, m.Np, 1), q1)
+    p.close()
+    ps.close()
