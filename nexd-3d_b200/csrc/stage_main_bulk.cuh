@@ -27,9 +27,9 @@
 
 namespace nexd_dev {
 
-template <int N>
+template <int N, int NPT = 1>
 struct MainBulkOrder {
-  using O = Order<N>;
+  using O = Order<N, NPT>;
   static constexpr int Np = O::Np, E = O::E;
   static constexpr int FT = EBlock<6 * kNMB, Np>::FS;  // floats per element: memory variables
   static constexpr int STH = E * FT;
@@ -48,24 +48,103 @@ struct MainBulkOrder {
   static constexpr int smem_floats() { return MBAR_OFF + 4; }
 };
 
-template <int N>
+template <int N, int NPT = 1>
 __device__ __forceinline__ void load_theta(const StageArgs& a, const Chunk& c, float* sTh, float* sTh2,
                                            uint32_t mbar) {
-  using B = MainBulkOrder<N>;
+  using B = MainBulkOrder<N, NPT>;
   const long long bt = eblock_chunk<6 * kNMB, B::Np>(a.ldt, c);
   const uint32_t nt = uint32_t(c.ne) * B::FT * 4;
   mbar_expect_tx(mbar, 2 * nt);
   bulk_load(sTh, a.th + bt, nt, mbar);
   bulk_load(sTh2, a.th2 + bt, nt, mbar);
 }
-template <int N>
+template <int N, int NPT = 1>
 __device__ __forceinline__ void store_theta(const StageArgs& a, const Chunk& c, const float* sTh, const float* sTh2) {
-  using B = MainBulkOrder<N>;
+  using B = MainBulkOrder<N, NPT>;
   const long long bt = eblock_chunk<6 * kNMB, B::Np>(a.ldt, c);
   const uint32_t nt = uint32_t(c.ne) * B::FT * 4;
   bulk_store(a.th + bt, sTh, nt);
   bulk_store(a.th2 + bt, sTh2, nt);
   bulk_commit();
+}
+
+// Update phase of one node of an anelastic element outside the NPML with its
+// memory variables in shared memory (ths / th2s at a stride of Np floats,
+// updated in place): Zener terms (src/timeloopMod.f90:426-461), point
+// sources, the receiver acceleration and the stage update of q; res holds
+// the node's residual of q (TVD: step-start q) and qown its interleaved own
+// values.  The operations and their order are those of finish_node.
+template <int Np, int MODE>
+__device__ __forceinline__ void finish_theta_smem(const StageArgs& a, int b, int e, long long node, int n, float* rq,
+                                                  const float* S, const float* res, float* ths, float* th2s,
+                                                  const float* qown) {
+  const float* ae = a.ael + (long long)e * 3 * kNMB;
+#pragma unroll
+  for (int l = 0; l < kNMB; ++l) {
+    const float wl = a.wlv[l];
+    float t[6], t2[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      t[j] = ths[(6 * l + j) * Np];
+      t2[j] = th2s[(6 * l + j) * Np];
+    }
+    const float c1 = ae[3 * l], c2 = ae[3 * l + 1], c3 = ae[3 * l + 2];
+    rq[0] += c3 * t[0] + c1 * (t[1] + t[2]);
+    rq[1] += c3 * t[1] + c1 * (t[2] + t[0]);
+    rq[2] += c3 * t[2] + c1 * (t[0] + t[1]);
+    rq[3] += c2 * t[3];
+    rq[4] += c2 * t[4];
+    rq[5] += c2 * t[5];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const float r = wl * (S[j] - t[j]);
+      const int o = (l * 6 + j) * Np;
+      float nt_;
+      if (MODE == MODE_LSERK) {
+        const float rr = a.ca * t2[j] + a.dt * r;
+        th2s[o] = rr;
+        nt_ = t[j] + a.cb * rr;
+      } else {
+        float tn;
+        if (a.stage_first) { th2s[o] = t[j]; tn = t[j]; } else { tn = t2[j]; }
+        nt_ = a.ca * tn + a.cb * (t[j] + a.dt * r);
+      }
+      ths[o] = nt_;
+    }
+  }
+  for (int s = a.src_head[e]; s >= 0; s = a.src_next[s]) {
+    if (a.src_batch[s] != b) continue;
+    const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
+    const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
+    const float* sp = a.src_pat + (long long)s * 9 * Np + n;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) rq[c] = fmaf(sp[c * Np], amp, rq[c]);
+  }
+  if (a.last_stage) {
+    const int slot = a.rec_slot[e];
+    if (slot >= 0) {
+      float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
+      ab[0] = rq[6];
+      ab[Np] = rq[7];
+      ab[2 * Np] = rq[8];
+    }
+  }
+  float* qo = a.q_out + (long long)b * 9 * a.ldq + node;
+  if (MODE == MODE_LSERK) {
+    float* rsg = a.res + eblock<9, Np>(a.ldq, b, e, n);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const float r = a.ca * res[c] + a.dt * rq[c];
+      __stcs(rsg + c * Np, r);
+      __stcs(qo + c * a.ldq, qown[c] + a.cb * r);
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const float base = (a.ca != 0.f) ? a.ca * res[c] : 0.f;
+      __stcs(qo + c * a.ldq, base + a.cb * (qown[c] + a.dt * rq[c]));
+    }
+  }
 }
 
 template <int N, int MODE>
@@ -318,76 +397,8 @@ __global__ void __launch_bounds__(256, 2) stage_main_bulk_kernel(const StageArgs
       atomicOr(a.flag, 8);
       ok = false;
     } else {
-      float* ths = sTh + le * B::FT + n;
-      float* th2s = sTh2 + le * B::FT + n;
-      const float* ae = a.ael + (long long)e * 3 * kNMB;
-#pragma unroll
-      for (int l = 0; l < kNMB; ++l) {
-        const float wl = a.wlv[l];
-        float t[6], t2[6];
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-          t[j] = ths[(6 * l + j) * Np];
-          t2[j] = th2s[(6 * l + j) * Np];
-        }
-        const float c1 = ae[3 * l], c2 = ae[3 * l + 1], c3 = ae[3 * l + 2];
-        rq[0] += c3 * t[0] + c1 * (t[1] + t[2]);
-        rq[1] += c3 * t[1] + c1 * (t[2] + t[0]);
-        rq[2] += c3 * t[2] + c1 * (t[0] + t[1]);
-        rq[3] += c2 * t[3];
-        rq[4] += c2 * t[4];
-        rq[5] += c2 * t[5];
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-          const float r = wl * (S[j] - t[j]);
-          const int o = (l * 6 + j) * Np;
-          float nt_;
-          if (MODE == MODE_LSERK) {
-            const float rr = a.ca * t2[j] + a.dt * r;
-            th2s[o] = rr;
-            nt_ = t[j] + a.cb * rr;
-          } else {
-            float tn;
-            if (a.stage_first) { th2s[o] = t[j]; tn = t[j]; } else { tn = t2[j]; }
-            nt_ = a.ca * tn + a.cb * (t[j] + a.dt * r);
-          }
-          ths[o] = nt_;
-        }
-      }
-      for (int s = a.src_head[e]; s >= 0; s = a.src_next[s]) {
-        if (a.src_batch[s] != b) continue;
-        const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
-        const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
-        const float* sp = a.src_pat + (long long)s * 9 * Np + n;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) rq[c] = fmaf(sp[c * Np], amp, rq[c]);
-      }
-      if (a.last_stage) {
-        const int slot = a.rec_slot[e];
-        if (slot >= 0) {
-          float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
-          ab[0] = rq[6];
-          ab[Np] = rq[7];
-          ab[2 * Np] = rq[8];
-        }
-      }
-      const float* qown = sQI + le * O::QE + n * QS;
-      float* qo = a.q_out + (long long)b * 9 * a.ldq + node;
-      if (MODE == MODE_LSERK) {
-        float* rsg = a.res + eblock<9, Np>(a.ldq, b, e, n);
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-          const float r = a.ca * res[c] + a.dt * rq[c];
-          __stcs(rsg + c * Np, r);
-          __stcs(qo + c * a.ldq, qown[c] + a.cb * r);
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-          const float base = (a.ca != 0.f) ? a.ca * res[c] : 0.f;
-          __stcs(qo + c * a.ldq, base + a.cb * (qown[c] + a.dt * rq[c]));
-        }
-      }
+      finish_theta_smem<Np, MODE>(a, b, e, node, n, rq, S, res, sTh + le * B::FT + n, sTh2 + le * B::FT + n,
+                                  sQI + le * O::QE + n * QS);
     }
     tc::fence_async_smem();  // this thread's writes to theta are seen by the bulk store
     prev = ch;
