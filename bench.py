@@ -244,7 +244,7 @@ def run_multimodel(args, grp, tmp, steps, warmup):
         return
     cpu = None
     if not args.no_cpu_baseline and grp.world == 1:
-        v, cores, sample = oracle_baseline(tmp, "twolayer")
+        v, cores, sample, _ = oracle_baseline(tmp, "twolayer")
         cpu = {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
     line = {
         "metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": grp.world, "steps": steps,
@@ -330,12 +330,13 @@ def summarize_clocks(path, device):
             "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def oracle_baseline(tmp, workload="twolayer", mesh=None, steps=CPU_STEPS, seed=None):
+def oracle_baseline(tmp, workload="twolayer", mesh=None, steps=CPU_STEPS, seed=None, warmup=0):
     """The CPU restatement of the reference solver (the oracle, FP32 like the
     reference's default CUSTOM_REAL) on the host cores, all OpenMP threads,
     over `steps` steps of the same workload (the mesh given, or one built
-    with the same generator, sizes and seed); the rate counts the step loop
-    only.  Returns (DOF-stage/s, threads, sample description)."""
+    with the same generator, sizes and seed), after `warmup` untimed steps;
+    the rate counts the timed step loop only.  Returns (DOF-stage/s, threads,
+    sample description, ms per step)."""
     lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
     lib.oracle_run.argtypes = [C.POINTER(_abi.NexdDesc), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_void_p, C.c_int]
     lib.oracle_loop_seconds.restype = C.c_double
@@ -357,6 +358,9 @@ def oracle_baseline(tmp, workload="twolayer", mesh=None, steps=CPU_STEPS, seed=N
     if workload == "cube":
         steps = max(steps, 20)
     tr = np.zeros((m.nrec, m.nt, 9, m.nbatch), dtype=np.float32, order="F")
+    if warmup > 0:
+        if lib.oracle_run(m.desc_ptr, 32, warmup, tr.ctypes.data_as(C.POINTER(C.c_float)), None, 0) != 0:
+            raise RuntimeError("oracle failed in the warm-up steps")
     t0 = time.perf_counter()
     st = lib.oracle_run(m.desc_ptr, 32, steps, tr.ctypes.data_as(C.POINTER(C.c_float)), None, 0)
     wall = time.perf_counter() - t0
@@ -367,7 +371,7 @@ def oracle_baseline(tmp, workload="twolayer", mesh=None, steps=CPU_STEPS, seed=N
     cores = os.cpu_count() or 1
     sample = (f"{steps} LSERK4 steps of the timed workload itself ({m.K} tets, N={m.N}, {m.nbatch} wavefield(s)), "
               f"FP32, {cores} OpenMP threads; step loop {el:.1f} s (set-up excluded, {wall:.1f} s wall in total)")
-    return units / el, cores, sample
+    return units / el, cores, sample, 1e3 * el / steps
 
 
 def main():
@@ -421,13 +425,14 @@ def main():
     try:
         if args.impl == "reference":
             if rank == 0:
-                v, cores, sample = oracle_baseline(tmp, args.workload, steps=CPU_STEPS)
+                # each step of this arm is one LSERK4 step of the whole workload on the host cores
+                v, cores, sample, ms = oracle_baseline(tmp, args.workload, steps=steps, warmup=warmup)
                 line = {"metric": metric, "value": v, "unit": "DOF-stage/s", "n_gpus": args.gpus, "steps": steps,
-                        "warmup": warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                        "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                         "config": {"workload": workload, "tets": wl["cells"][0] * wl["cells"][1] * wl["cells"][2] * 6
                                    if wl["cells"] else None, "N": wl["N"], "integrator": "LSERK4 (5 stages)",
-                                   "sample": f"{CPU_STEPS} steps of this workload (see cpu_baseline)"},
+                                   "sample": f"{steps} steps of this workload after {warmup} untimed (see cpu_baseline)"},
                         "impl": "reference",
                         "cpu_baseline": {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port",
                                          "sample": sample},
@@ -535,7 +540,7 @@ def main():
         s.close()  # frees the device state before the CPU leg
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            v, cores, sample = oracle_baseline(tmp, args.workload, mesh=mesh)
+            v, cores, sample, _ = oracle_baseline(tmp, args.workload, mesh=mesh)
             cpu = {"value": v, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
         clocks = summarize_clocks(clk_file, local) if clk else None
         state_gb = (2 * 9 + 9 + 2 * 6 * mesh.desc.nMB) * mesh.K * mesh.Np * 4 * nb / 1e9

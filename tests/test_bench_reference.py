@@ -33,6 +33,9 @@ def test_reference_arm_under_two_ranks():
     d = lines[0]
     assert d["impl"] == "reference" and d["metric"] == "DOF-stage updates/s" and d["unit"] == "DOF-stage/s"
     assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 2
+    # the requested steps were timed (after the requested untimed ones) and their time is reported
+    assert d["steps"] == 1 and d["warmup"] == 3 and d["ms_per_step"] > 0
+    assert "1 LSERK4 steps" in d["cpu_baseline"]["sample"]
     # the same workload as the GPU arm: the full 192,000-tet model, not a smaller sample
     assert d["config"]["workload"] == "twolayer_anelastic_npml_192k_tets_N4_lserk4" and d["config"]["tets"] == 192000
     cb = d["cpu_baseline"]
