@@ -77,8 +77,8 @@ __device__ __forceinline__ void store_theta(const StageArgs& a, const Chunk& c, 
 template <int Np, int MODE>
 __device__ __forceinline__ void finish_theta_smem(const StageArgs& a, int b, int e, long long node, int n, float* rq,
                                                   const float* S, const float* res, float* ths, float* th2s,
-                                                  const float* qown) {
-  const float* ae = a.ael + (long long)e * 3 * kNMB;
+                                                  const float* qown, const ElemScalars<true>& es) {
+  const float* ae = es.ae;
 #pragma unroll
   for (int l = 0; l < kNMB; ++l) {
     const float wl = a.wlv[l];
@@ -112,7 +112,7 @@ __device__ __forceinline__ void finish_theta_smem(const StageArgs& a, int b, int
       ths[o] = nt_;
     }
   }
-  for (int s = a.src_head[e]; s >= 0; s = a.src_next[s]) {
+  for (int s = es.src; s >= 0; s = a.src_next[s]) {
     if (a.src_batch[s] != b) continue;
     const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
     const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
@@ -121,7 +121,7 @@ __device__ __forceinline__ void finish_theta_smem(const StageArgs& a, int b, int
     for (int c = 0; c < 9; ++c) rq[c] = fmaf(sp[c * Np], amp, rq[c]);
   }
   if (a.last_stage) {
-    const int slot = a.rec_slot[e];
+    const int slot = es.slot;
     if (slot >= 0) {
       float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
       ab[0] = rq[6];
@@ -234,6 +234,8 @@ __global__ void __launch_bounds__(256, 2) stage_main_bulk_kernel(const StageArgs
     if (tid == 0 && !first) store_theta<N>(a, prev, sTh, sTh2);
     const bool active = le < ne;
     const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
+    ElemScalars<true> es;
+    es.load(a, b, e0 + (active ? le : 0));
     // residual of q (LSERK) or step-start q (TVD) of this node
     float res[9];
     if (active) {
@@ -398,7 +400,7 @@ __global__ void __launch_bounds__(256, 2) stage_main_bulk_kernel(const StageArgs
       ok = false;
     } else {
       finish_theta_smem<Np, MODE>(a, b, e, node, n, rq, S, res, sTh + le * B::FT + n, sTh2 + le * B::FT + n,
-                                  sQI + le * O::QE + n * QS);
+                                  sQI + le * O::QE + n * QS, es);
     }
     tc::fence_async_smem();  // this thread's writes to theta are seen by the bulk store
     prev = ch;

@@ -96,6 +96,26 @@ __device__ __forceinline__ uint32_t bulk_bytes(long long base, long long cnt) {
   return uint32_t((((base + cnt + 3) & ~3LL) - (base & ~3LL)) * 4);
 }
 
+// Per-element scalars of the update phase (first source, receiver slot on
+// the last stage, Zener coefficients) and the NPML switch, loaded when the
+// chunk starts: read where they are used, each is a dependent global load
+// whose latency the block (one per SM) would wait out once per chunk.
+template <bool ATT>
+struct ElemScalars {
+  int src, slot;
+  bool off;
+  float ae[ATT ? 3 * kNMB : 1];
+  __device__ __forceinline__ void load(const StageArgs& a, int b, int e) {
+    src = __ldg(a.src_head + e);
+    slot = a.last_stage ? __ldg(a.rec_slot + e) : -1;
+    off = a.pml_off[b] != 0;
+    if (ATT) {
+#pragma unroll
+      for (int j = 0; j < 3 * kNMB; ++j) ae[j] = __ldg(a.ael + (long long)e * 3 * kNMB + j);
+    }
+  }
+};
+
 // First float of chunk c's range in an element-blocked array of F fields.
 template <int F, int Np>
 __device__ __forceinline__ long long eblock_chunk(long long ld, const Chunk& c) {
@@ -233,10 +253,10 @@ __device__ __forceinline__ void pml_update_smem(const StageArgs& a, bool off, co
 template <int Np, bool ATT, int MODE>
 __device__ __forceinline__ void finish_node_smem(const StageArgs& a, int b, int e, long long node, float* rq,
                                                  const float* S, float* rs, int rstride, float* ths, float* th2s,
-                                                 const float* qown, int qstride) {
+                                                 const float* qown, int qstride, const ElemScalars<ATT>& es) {
   const int n = int(node - (long long)e * Np);
   if (ATT) {
-    const float* ae = a.ael + (long long)e * 3 * kNMB;
+    const float* ae = es.ae;
 #pragma unroll
     for (int l = 0; l < kNMB; ++l) {
       const float wl = a.wlv[l];
@@ -271,7 +291,7 @@ __device__ __forceinline__ void finish_node_smem(const StageArgs& a, int b, int 
       }
     }
   }
-  for (int s = a.src_head[e]; s >= 0; s = a.src_next[s]) {
+  for (int s = es.src; s >= 0; s = a.src_next[s]) {
     if (a.src_batch[s] != b) continue;
     const int sidx = a.nspt == 1 ? 0 : min(a.stage, a.nspt - 1);
     const float amp = a.stf[((long long)s * a.nt + (*a.it_dev - 1)) * a.nspt + sidx];
@@ -280,7 +300,7 @@ __device__ __forceinline__ void finish_node_smem(const StageArgs& a, int b, int 
     for (int c = 0; c < 9; ++c) rq[c] = fmaf(sp[c * Np], amp, rq[c]);
   }
   if (a.last_stage) {
-    const int slot = a.rec_slot[e];
+    const int slot = es.slot;
     if (slot >= 0) {
       float* ab = a.abuf + ((long long)b * a.nslot + slot) * 3 * Np + n;
       ab[0] = rq[6];
@@ -402,6 +422,8 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
     if (wn < nwork) cn = chunk_of<E>(a, wn, nchunk);
     const bool active = le < ne;
     const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
+    ElemScalars<ATT> es;
+    es.load(a, b, e0 + (active ? le : 0));
     if (wn < nwork) {
       const int wnn = wn + gridDim.x;
       Chunk cnn;
@@ -442,7 +464,7 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
       float F[9], G[9], H[9];
       elastic_fluxes(g, qv, F, G, H);
       const float* ps = sPrf + int(((long long)e0 * 9 * Np) & 3) + le * 9 * Np + n;
-      pml_update_smem<Np, MODE>(a, a.pml_off[b] != 0, ps, sAux + le * B::FA + n, sAux2 + le * B::FA + n, F, G, H);
+      pml_update_smem<Np, MODE>(a, es.off, ps, sAux + le * B::FA + n, sAux2 + le * B::FA + n, F, G, H);
       float2* cf = reinterpret_cast<float2*>(sCF + le * O::CFE + n * CS);
       float r[10], sv[10], t[10];
 #pragma unroll
@@ -574,7 +596,7 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
         rstride = B::QR;
       }
       finish_node_smem<Np, ATT, MODE>(a, b, e, node, rq, S, rs, rstride, sTh + le * B::FT + n,
-                                      sTh2 + le * B::FT + n, sQF + le * Np + n, O::QF);
+                                      sTh2 + le * B::FT + n, sQF + le * Np + n, O::QF, es);
     } else {
       atomicOr(a.flag, 8);
     }
