@@ -524,19 +524,30 @@ def main():
         kinds = [k for k in ("stage_main", "stage_pml") if prof[k]["launches"] > 0]
         nb = mesh.nbatch
         dom = max(kinds, key=lambda k: prof[k]["ms"])
-        per_launch_ms = prof[dom]["ms"] / prof[dom]["launches"]
-        abytes = algorithmic_bytes(mesh, dom, prof[dom]["elements"]) * nb
-        achieved = abytes / (per_launch_ms * 1e-3) / 1e9
-        traffic = None
         ckinds = s.contraction()[0]
         tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-        if os.path.exists(tp):
-            try:
-                kind = ckinds["npml" if dom == "stage_pml" else "rest"]
-                t = json.load(open(tp)).get(workload, {}).get(f"{dom}/{kind}")
-                traffic = None if t is None else float(t)
-            except Exception:
-                traffic = None
+
+        def kernel_roofline(k):
+            # algorithmic bytes per launch / mean launch time; DRAM traffic per launch from the ncu capture
+            ms = prof[k]["ms"] / prof[k]["launches"]
+            ab = algorithmic_bytes(mesh, k, prof[k]["elements"]) * nb
+            tr = None
+            if os.path.exists(tp):
+                try:
+                    t = json.load(open(tp)).get(workload, {}).get(f"{k}/{ckinds['npml' if k == 'stage_pml' else 'rest']}")
+                    tr = None if t is None else float(t)
+                except Exception:
+                    tr = None
+            return ms, ab, ab / (ms * 1e-3) / 1e9, tr
+
+        per_launch_ms, abytes, achieved, traffic = kernel_roofline(dom)
+        per_kernel = {}
+        for k in kinds:
+            ms_k, ab_k, ach_k, tr_k = kernel_roofline(k)
+            per_kernel[k] = {"kernel_kind": ckinds["npml" if k == "stage_pml" else "rest"], "achieved": ach_k,
+                             "frac": ach_k / peak, "traffic": tr_k, "algorithmic_bytes_per_launch": ab_k,
+                             "avg_launch_ms": ms_k, "share_of_stage_time": prof[k]["ms"] /
+                             sum(prof[j]["ms"] for j in kinds)}
         s.close()  # frees the device state before the CPU leg
         cpu = None
         if not args.no_cpu_baseline and world == 1:
@@ -561,7 +572,8 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": per_launch_ms},
+                         "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": per_launch_ms,
+                         "per_kernel": per_kernel},
             "kernels": {k: {"launches": prof[k]["launches"], "ms": round(prof[k]["ms"], 3)}
                         for k in ("record", "stage_pml", "stage_main")},
             "per_launch_pass_ms_per_step": prof["span_ms"] / steps,
