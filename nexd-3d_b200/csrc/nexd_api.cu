@@ -383,7 +383,7 @@ bool bulk_supported(int N, bool att, int cls) {
 }
 
 // Threads per block of a kernel kind.
-int kind_threads(int) { return 256; }
+int kind_threads(int kind, bool pml) { return (kind == KIND_BULK && pml) ? kBulkThreads : 256; }
 
 // Floats per element of an element-blocked array of F fields: F x Np
 // padded to a multiple of 4 (EBlock in stage_kernel.cuh).
@@ -539,7 +539,7 @@ int configure_launch(nexd_ctx* c) {
     if (!fn) return set_err(c, NEXD_ERR_UNSUPPORTED, "no stage kernel for this order and contraction");
     CUDA_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
-    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kind_threads(c->kind[which]), smem));
+    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kind_threads(c->kind[which], pmlk), smem));
     if (per_sm < 1) return set_err(c, NEXD_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
     const int nel = pmlk ? c->Kpml : c->K - c->Kpml;
     const long long work = (long long)((nel + E - 1) / E) * c->nbatch;
@@ -1074,7 +1074,7 @@ void launch_class(nexd_ctx* c, StageArgs& a, bool pml) {
     f<<<grid, 256, sm, c->stream>>>(a);
   } else if (c->kind[cls] == KIND_BULK && pml) {
     KernelFn f = pick_bulk_kernel(c->N, c->att, mode, smem);
-    f<<<grid, 256, sm, c->stream>>>(a);
+    f<<<grid, kBulkThreads, sm, c->stream>>>(a);
   } else if (c->kind[cls] == KIND_BULK && c->att) {
     KernelFn f = pick_main_bulk_kernel(c->N, mode, smem);
     f<<<grid, 256, sm, c->stream>>>(a);

@@ -300,12 +300,13 @@ __device__ __forceinline__ Chunk chunk_of(const StageArgs& a, int w, int nchunk)
 
 // Asynchronous copies of one chunk's element records (16-byte copies), own
 // wavefield (field-major), the connectivity of the chunk after it (`next`,
-// -1 for none) and the chunk's own face codes.  No commit.
+// -1 for none) and the chunk's own face codes, shared by threads
+// t0 .. t0 + nt - 1 (default: the whole block).  No commit.
 template <class O>
 __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, float* bGeo, float* bQ, int* bIds,
-                                           const Chunk* next) {
+                                           const Chunk* next, int t0 = -1, int nt = 0) {
   constexpr int Np = O::Np, E = O::E;
-  const int tid = threadIdx.x, nth = blockDim.x;
+  const int tid = t0 < 0 ? int(threadIdx.x) : t0, nth = t0 < 0 ? int(blockDim.x) : nt;
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
   for (int i = tid; i < c.ne * (GEO_STRIDE / 4); i += nth)
     cp_async16(bGeo + (i / (GEO_STRIDE / 4)) * O::GSTR + 4 * (i % (GEO_STRIDE / 4)),
@@ -330,12 +331,14 @@ __device__ __forceinline__ void issue_main(const StageArgs& a, const Chunk& c, f
 
 // Asynchronous gather of the neighbour face traces of one chunk's interior
 // faces through the face patterns, using its connectivity `ids` (staged one
-// chunk earlier): face nodes [lo, hi) of the chunk (hi < 0: all).  No commit.
+// chunk earlier): face nodes [lo, hi) of the chunk (hi < 0: all), shared by
+// threads t0 .. t0 + nt - 1 (default: the whole block).  No commit.
 template <class O>
 __device__ __forceinline__ void issue_traces(const StageArgs& a, const Chunk& c, const int* ids, float* bTr,
-                                             const unsigned char* pat, int lo = 0, int hi = -1) {
+                                             const unsigned char* pat, int lo = 0, int hi = -1, int t0 = -1,
+                                             int nt = 0) {
   constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF;
-  const int tid = threadIdx.x, nth = blockDim.x;
+  const int tid = t0 < 0 ? int(threadIdx.x) : t0, nth = t0 < 0 ? int(blockDim.x) : nt;
   const float* qin = a.q_in + (long long)c.b * 9 * a.ldq;
   const int end = hi < 0 ? c.ne * NF : hi;
   for (int i = lo + tid; i < end; i += nth) {

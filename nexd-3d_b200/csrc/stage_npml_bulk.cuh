@@ -325,8 +325,17 @@ __device__ __forceinline__ void finish_node_smem(const StageArgs& a, int b, int 
   }
 }
 
+// Threads of the bulk-copy NPML kernel: 8 compute warps (the node mapping of
+// stage_kernel) and one producer warp that issues every copy of the chunk
+// pipeline -- the next chunk's records, wavefield, connectivity and
+// neighbour-trace gather (cp.async) and the bulk loads and stores of buffers
+// A and B -- so the compute warps spend no issue slots on them and never wait
+// at a barrier for a thread that is issuing copies.
+constexpr int kCompute = 256;
+constexpr int kBulkThreads = kCompute + 32;
+
 template <int N, bool ATT, int MODE>
-__global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs a) {
+__global__ void __launch_bounds__(kBulkThreads, 1) stage_npml_bulk_kernel(const StageArgs a) {
   using O = Order<N>;
   using B = BulkOrder<N>;
   constexpr int Np = O::Np, NpF = O::NpF, NF = O::NF, E = O::E, CS = O::CS;
@@ -347,6 +356,8 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
   const uint32_t mbarA = tc::smem_u32(mbars), mbarB = tc::smem_u32(mbars + 1);
 
   const int tid = threadIdx.x;
+  const bool producer = tid >= kCompute;
+  const int lane = tid & 31;
   for (int i = tid; i < Np * Np; i += blockDim.x) {
     reinterpret_cast<float2*>(sD)[i] = make_float2(a.D[i], a.D[Np * Np + i]);
     sD[2 * Np * Np + i] = a.D[2 * Np * Np + i];
@@ -360,19 +371,21 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
   const int nel = a.e_end - a.e_begin;
   const int nchunk = (nel + E - 1) / E;
   const int nwork = nchunk * a.nbatch;
-  int le, n;
-  if constexpr (O::WARP_ALIGNED) {
-    if (tid < E * 32) {
-      le = tid >> 5;
-      n = tid & 31;
+  int le = E, n = 0;  // the producer warp holds no node
+  if (!producer) {
+    if constexpr (O::WARP_ALIGNED) {
+      if (tid < E * 32) {
+        le = tid >> 5;
+        n = tid & 31;
+      } else {
+        const int r = tid - E * 32;
+        le = r / (Np - 32);
+        n = 32 + r - le * (Np - 32);
+      }
     } else {
-      const int r = tid - E * 32;
-      le = r / (Np - 32);
-      n = 32 + r - le * (Np - 32);
+      le = tid / Np;
+      n = tid - le * Np;
     }
-  } else {
-    le = tid / Np;
-    n = tid - le * Np;
   }
   int w = blockIdx.x;
   if (w >= nwork) return;
@@ -388,17 +401,22 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
       ids0[ee * 12 + k] = k < 4 ? reinterpret_cast<const int*>(a.nbr)[4 * (c0.e0 + ee) + k]
                                 : reinterpret_cast<const int*>(a.fcode)[4 * (c0.e0 + ee) + k - 4];
     }
-    if (tid == 0) {
+    if (tid == kCompute) {
       tc::mbar_init(mbarA, 1);
       tc::mbar_init(mbarB, 1);
       fence_mbar_init();
     }
     __syncthreads();
-    if (tid == 0) {
-      load_state_a<N>(a, c0, sAux, sAux2, sPrf, mbarA);
-      load_state_b<N, ATT, MODE>(a, c0, sRes, sTh, sTh2, mbarB);
+    if (producer) {
+      if (lane == 0) {
+        load_state_a<N>(a, c0, sAux, sAux2, sPrf, mbarA);
+        load_state_b<N, ATT, MODE>(a, c0, sRes, sTh, sTh2, mbarB);
+      }
+      issue_main<O>(a, c0, sBuf, sBuf + O::SGEO, reinterpret_cast<int*>(sBuf + O::SGEO + O::SQF + O::STR),
+                    wn < nwork ? &c1 : nullptr, lane, 32);
+      issue_traces<O>(a, c0, ids0, sBuf + O::SGEO + O::SQF, sPat, 0, -1, lane, 32);
+      cp_async_commit();
     }
-    issue_chunk<O>(a, c0, ids0, sBuf, wn < nwork ? &c1 : nullptr, sPat);
   }
 
   bool ok = true;
@@ -413,87 +431,103 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
     const float* sTr = buf + O::SGEO + O::SQF;
     const float* sQF = buf + O::SGEO + int(((long long)e0 * Np) & 3);
     const int* sIds = reinterpret_cast<const int*>(sTr + O::STR);
-    cp_async_wait_all();
+    cp_async_wait_all();  // the producer's copies of this chunk (the compute warps have none)
     __syncthreads();  // (1) records, wavefield and traces in `buf`; the previous chunk's buffer B is final
-    // the previous chunk's residual and memory variables go back to global memory
-    if (tid == 0 && !first) store_state_b<N, ATT, MODE>(a, prev, sRes, sTh, sTh2);
     const int wn = w + gridDim.x;
     Chunk cn;
     if (wn < nwork) cn = chunk_of<E>(a, wn, nchunk);
+    float* nbuf = sBuf + (p ^ 1) * O::BUF;
+    bool okA = true;
     const bool active = le < ne;
     const long long node = (long long)(e0 + (active ? le : 0)) * Np + n;
     ElemScalars<ATT> es;
-    es.load(a, b, e0 + (active ? le : 0));
-    if (wn < nwork) {
-      const int wnn = wn + gridDim.x;
-      Chunk cnn;
-      if (wnn < nwork) cnn = chunk_of<E>(a, wnn, nchunk);
-      issue_chunk_head<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, wnn < nwork ? &cnn : nullptr, sPat);
-    }
-    // ---- face amplitudes ---------------------------------------------------------
-    for (int i = tid; i < ne * NF; i += blockDim.x) {
-      const int ee = i / NF, j = i - ee * NF;
-      const int f = j / NpF, fi = j - f * NpF;
-      const float* g = sGeo + ee * O::GSTR;
-      const int code = sIds[ee * 12 + 8 + f];
-      const int own = sPat[f * NpF + fi];
-      const float* qo = sQF + ee * Np + own;
-      float dq[9];
-      const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, O::QF, dq);
-      float ap, as1, as2;
-      face_amplitudes(g, f, dq, free_face, ap, as1, as2);
-      const float fs = g[G_FS + f];
-      float* am = sAmp + ee * O::AE + f * 2 * O::NPAIR + fi;
-      am[0] = ap * fs;
-      am[O::NFP] = as1 * fs;
-      am[2 * O::NFP] = as2 * fs;
-    }
-    if (wn < nwork) issue_trace_slice<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, sPat, 1);
-    // buffer B was read by its store long ago: refill it with this chunk's state
-    if (tid == 0 && !first) {
-      bulk_wait_read();
-      load_state_b<N, ATT, MODE>(a, ch, sRes, sTh, sTh2, mbarB);
-    }
-    // ---- NPML: auxiliary update (in place) and contravariant modified fluxes -------
-    const bool okA = tc::mbar_wait(mbarA, phase);
-    if (active && okA) {
-      const float* g = sGeo + le * O::GSTR;
-      float qv[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) qv[c] = sQF[c * O::QF + le * Np + n];
-      float F[9], G[9], H[9];
-      elastic_fluxes(g, qv, F, G, H);
-      const float* ps = sPrf + int(((long long)e0 * 9 * Np) & 3) + le * 9 * Np + n;
-      pml_update_smem<Np, MODE>(a, es.off, ps, sAux + le * B::FA + n, sAux2 + le * B::FA + n, F, G, H);
-      float2* cf = reinterpret_cast<float2*>(sCF + le * O::CFE + n * CS);
-      float r[10], sv[10], t[10];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        r[i] = g[G_RX] * F[i] + g[G_RY] * G[i] + g[G_RZ] * H[i];
-        sv[i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
-        t[i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
+    if (producer) {
+      // the previous chunk's residual and memory variables go back, this
+      // chunk's come in; the next chunk's records, wavefield and connectivity start
+      if (lane == 0 && !first) {
+        store_state_b<N, ATT, MODE>(a, prev, sRes, sTh, sTh2);
+        bulk_wait_read();
+        load_state_b<N, ATT, MODE>(a, ch, sRes, sTh, sTh2, mbarB);
       }
-      r[9] = ATT ? qv[6] : 0.f;
-      sv[9] = ATT ? qv[7] : 0.f;
-      t[9] = ATT ? qv[8] : 0.f;
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        cf[j] = make_float2(r[2 * j], r[2 * j + 1]);
-        cf[5 + j] = make_float2(sv[2 * j], sv[2 * j + 1]);
-        cf[10 + j] = make_float2(t[2 * j], t[2 * j + 1]);
+      if (wn < nwork) {
+        const int wnn = wn + gridDim.x;
+        Chunk cnn;
+        if (wnn < nwork) cnn = chunk_of<E>(a, wnn, nchunk);
+        issue_main<O>(a, cn, nbuf, nbuf + O::SGEO, reinterpret_cast<int*>(nbuf + O::SGEO + O::SQF + O::STR),
+                      wnn < nwork ? &cnn : nullptr, lane, 32);
       }
+    } else {
+      es.load(a, b, e0 + (active ? le : 0));
+      // ---- face amplitudes ---------------------------------------------------------
+      for (int i = tid; i < ne * NF; i += kCompute) {
+        const int ee = i / NF, j = i - ee * NF;
+        const int f = j / NpF, fi = j - f * NpF;
+        const float* g = sGeo + ee * O::GSTR;
+        const int code = sIds[ee * 12 + 8 + f];
+        const int own = sPat[f * NpF + fi];
+        const float* qo = sQF + ee * Np + own;
+        float dq[9];
+        const bool free_face = face_jump<NpF>(a, b, code, fi, sTr + i * 9, qo, O::QF, dq);
+        float ap, as1, as2;
+        face_amplitudes(g, f, dq, free_face, ap, as1, as2);
+        const float fs = g[G_FS + f];
+        float* am = sAmp + ee * O::AE + f * 2 * O::NPAIR + fi;
+        am[0] = ap * fs;
+        am[O::NFP] = as1 * fs;
+        am[2 * O::NFP] = as2 * fs;
+      }
+      // ---- NPML: auxiliary update (in place) and contravariant modified fluxes -------
+      okA = tc::mbar_wait(mbarA, phase);
+      if (active && okA) {
+        const float* g = sGeo + le * O::GSTR;
+        float qv[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) qv[c] = sQF[c * O::QF + le * Np + n];
+        float F[9], G[9], H[9];
+        elastic_fluxes(g, qv, F, G, H);
+        const float* ps = sPrf + int(((long long)e0 * 9 * Np) & 3) + le * 9 * Np + n;
+        pml_update_smem<Np, MODE>(a, es.off, ps, sAux + le * B::FA + n, sAux2 + le * B::FA + n, F, G, H);
+        float2* cf = reinterpret_cast<float2*>(sCF + le * O::CFE + n * CS);
+        float r[10], sv[10], t[10];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+          r[i] = g[G_RX] * F[i] + g[G_RY] * G[i] + g[G_RZ] * H[i];
+          sv[i] = g[G_SX] * F[i] + g[G_SY] * G[i] + g[G_SZ] * H[i];
+          t[i] = g[G_TX] * F[i] + g[G_TY] * G[i] + g[G_TZ] * H[i];
+        }
+        r[9] = ATT ? qv[6] : 0.f;
+        sv[9] = ATT ? qv[7] : 0.f;
+        t[9] = ATT ? qv[8] : 0.f;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+          cf[j] = make_float2(r[2 * j], r[2 * j + 1]);
+          cf[5 + j] = make_float2(sv[2 * j], sv[2 * j + 1]);
+          cf[10 + j] = make_float2(t[2 * j], t[2 * j + 1]);
+        }
+      }
+      tc::fence_async_smem();  // this thread's writes to buffer A are seen by the bulk store
     }
-    tc::fence_async_smem();  // this thread's writes to buffer A are seen by the bulk store
     if (__syncthreads_or(!okA)) {  // (2) amplitudes and rows are in shared memory; buffer A is final
       ok = false;
       break;
     }
-    if (tid == 0) store_state_a<N>(a, ch, sAux, sAux2);
-    if (wn < nwork) issue_trace_slice<O>(a, cn, sIds, sBuf + (p ^ 1) * O::BUF, sPat, 2);
-    if (!active) {
-      // idle threads of a partial chunk: thread 0 is never idle, so nothing else to do
+    if (producer) {
+      // buffer A goes back and is refilled with the next chunk's; the next chunk's traces
+      if (lane == 0) {
+        store_state_a<N>(a, ch, sAux, sAux2);
+        if (wn < nwork) {
+          bulk_wait_read();
+          load_state_a<N>(a, cn, sAux, sAux2, sPrf, mbarA);
+        }
+      }
+      if (wn < nwork) issue_traces<O>(a, cn, sIds, nbuf + O::SGEO + O::SQF, sPat, 0, -1, lane, 32);
+      cp_async_commit();
       prev = ch;
       continue;
+    }
+    if (!active) {
+      prev = ch;
+      continue;  // idle threads of a partial chunk
     }
 
     const int e = e0 + le;
@@ -544,11 +578,6 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
           vgrad[c * 3 + 2] = g[G_RZ] * vr[c] + g[G_SZ] * vs3[c] + g[G_TZ] * vt3[c];
         }
       }
-    }
-    // buffer A was read by its store during the volume loop: refill it with the next chunk's
-    if (tid == 0 && wn < nwork) {
-      bulk_wait_read();
-      load_state_a<N>(a, cn, sAux, sAux2, sPrf, mbarA);
     }
     float sig_an[6];
 #pragma unroll
@@ -603,9 +632,9 @@ __global__ void __launch_bounds__(256, 1) stage_npml_bulk_kernel(const StageArgs
     tc::fence_async_smem();  // this thread's writes to buffer B are seen by the bulk store
     prev = ch;
   }
-  __syncthreads();
-  if (tid == 0) {
-    if (ok) {
+  const bool all_ok = __syncthreads_and(ok);
+  if (tid == kCompute) {
+    if (all_ok) {
       store_state_b<N, ATT, MODE>(a, prev, sRes, sTh, sTh2);
     } else {
       // a load did not complete in time: wait once more, again bounded, for
