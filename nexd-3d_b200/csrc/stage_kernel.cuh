@@ -369,26 +369,6 @@ __device__ __forceinline__ void issue_chunk(const StageArgs& a, const Chunk& c, 
   cp_async_commit();
 }
 
-// The trace gather of a chunk split into three slices of its face nodes,
-// issued at three points of the chunk before it (each its own commit group),
-// so the gathers overlap the compute phases (used by the bulk-copy stage
-// kernels: 1.3 % shorter NPML launches than one gather burst).
-constexpr int kTraceSlices = 3;
-template <class O>
-__device__ __forceinline__ void issue_trace_slice(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
-                                                  const unsigned char* pat, int s) {
-  const int n = c.ne * O::NF;
-  issue_traces<O>(a, c, ids, buf + O::SGEO + O::SQF, pat, s * n / kTraceSlices, (s + 1) * n / kTraceSlices);
-  cp_async_commit();
-}
-// Records, wavefield and connectivity of a chunk plus its first trace slice.
-template <class O>
-__device__ __forceinline__ void issue_chunk_head(const StageArgs& a, const Chunk& c, const int* ids, float* buf,
-                                                 const Chunk* next, const unsigned char* pat) {
-  issue_main<O>(a, c, buf, buf + O::SGEO, reinterpret_cast<int*>(buf + O::SGEO + O::SQF + O::STR), next);
-  issue_trace_slice<O>(a, c, ids, buf, pat, 0);
-}
-
 // Memory variables per mechanism set: the reference's nMB = 3 (src/constants.h:36).
 constexpr int kNMB = 3;
 

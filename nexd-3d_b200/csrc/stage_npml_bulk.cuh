@@ -13,18 +13,21 @@
 // computes nothing meanwhile.  Here each array's chunk range -- element-
 // blocked, each element's block 16-byte aligned (eblock), so one contiguous
 // range per array -- moves between global and shared memory as one 1-D bulk
-// copy issued by one thread (cp.async.bulk; loads complete on an mbarrier,
-// stores in bulk groups; no multicast), while the block computes; the
-// threads update the state in place in shared memory:
+// copy (cp.async.bulk; loads complete on an mbarrier, stores in bulk groups;
+// no multicast), and the threads update the state in place in shared memory:
 //
 //   buffer A   F', G', H', their residuals (TVD: step-start values) and the
-//              9 damping profiles of the chunk, used in the NPML phase;
-//              stored back right after that phase, refilled with the next
-//              chunk's after the volume loop
+//              9 damping profiles of the chunk, used in the NPML phase
 //   buffer B   the LSERK residual of q (TVD: the step-start q, read only),
 //              the memory variables and their residuals, used in the update
-//              phase; stored back at the start of the next chunk, refilled
-//              with that chunk's after its face phase
+//              phase
+//
+// The block is warp-specialised: 8 compute warps and one producer warp (see
+// kCompute below).  Per chunk the producer stores the previous chunk's B and
+// loads this chunk's once the store has read it, and starts the next chunk's
+// records, wavefield and connectivity (cp.async); after the compute warps'
+// NPML phase (second barrier) it stores A, loads the next chunk's A and
+// gathers the next chunk's neighbour traces.  The compute warps only compute.
 //
 // The profiles and the TVD step-start q keep their unpadded layouts: their
 // ranges are widened to 16-byte boundaries for the loads (the arrays carry 4
