@@ -138,6 +138,8 @@ def run_partitions(args, grp, tmp, steps, warmup, cells, workload):
     ps = Partitions(mesh.desc_ptr, args.parts, centroids=element_centroids(mesh))
     p = PartitionedSolver(ps, nrec_total=mesh.nrec)
     p0 = p.solvers[0]
+    for x in p.solvers:  # each partition's kernels chosen like the whole mesh's (autotune by default)
+        x.set_contraction(args.contraction if (mesh.N == 4 or args.contraction != "bf16x3") else "fp32")
     p.run(1, warmup)
     torch.cuda.synchronize()
     clk_file = os.path.join(tmp, "clocks.csv")
@@ -168,6 +170,7 @@ def run_partitions(args, grp, tmp, steps, warmup, cells, workload):
         "data": "synthetic (seeded two-layer model, seeded source)",
         "config": {"workload": workload, "tets": mesh.K, "N": mesh.N, "partitions": args.parts,
                    "partition_tets": [x.K for x in p.solvers], "integrator": "LSERK4 (5 stages)",
+                   "kernels_per_class": [x.contraction()[0] for x in p.solvers],
                    "timed": "partitions interleaved stage by stage in one stream, launched kernel by kernel"},
         "halo": {"bytes_per_stage": hbytes, "ms_per_stage": halo_ms_stage,
                  "share_of_step": kinds["halo"]["ms"] / max(1e-9, sum(v["ms"] for v in kinds.values())),
