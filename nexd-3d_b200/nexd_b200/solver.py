@@ -95,8 +95,10 @@ class Solver:
 
     def set_contraction(self, mode):
         """Element contraction arithmetic: "fp32" (CUDA cores, default),
-        "bf16x3" (tcgen05 tensor cores, split BF16, FP32 accumulation) or
-        "auto" (the faster of the two per element class, timed on this mesh)."""
+        "bf16x3" (tcgen05 tensor cores, split BF16, FP32 accumulation),
+        "fp32_pairs" (the node-pair FP32 kernel outside the NPML) or "auto"
+        (per element class the fastest candidate kernel, timed on this mesh;
+        the bulk-copy kernels are candidates too)."""
         m = {"fp32": _abi.NEXD_CONTRACT_FP32, "bf16x3": _abi.NEXD_CONTRACT_BF16X3,
              "auto": _abi.NEXD_CONTRACT_AUTO, "fp32_pairs": _abi.NEXD_CONTRACT_FP32_PAIRS}.get(mode, mode)
         st = _abi.gpu_lib().nexd_set_contraction(self._ctx, m)

@@ -194,3 +194,35 @@ def test_group_autotune_chooses_between_modes(tmp_path, solver_mod, oracle):
         to, fo = run_oracle(oracle, m, 64, want_field=True)
         assert rel_l2(s.field(), fo[..., 0]) < 1e-4
     g.close()
+
+
+def test_group_with_bulk_copy_kernels_equals_member_runs(tmp_path, solver_mod):
+    """Members on the bulk-copy stage kernels (an NPML model at N=4 with both
+    element classes pinned to them; an anelastic model at N=3 without NPML,
+    its elements on the bulk-copy kernel of the rest) stepped together as
+    graph branches give their own runs bit for bit."""
+    d1 = str(tmp_path / "npml4")
+    synth.write_twolayer(d1, cells=(8, 8, 4), nt=30, nrec=4, src_depth=(900.0, 900.0))
+    d2 = str(tmp_path / "tl3")
+    synth.write_twolayer(d2, cells=(6, 6, 3), nt=30, nrec=4, src_depth=(900.0, 900.0), pml=False, src_seed=5)
+    specs = [(Mesh(d1, N=4, stf_stage_time=True), ("fp32_bulk", "fp32_bulk")),
+             (Mesh(d2, N=3, stf_stage_time=True), ("fp32", "fp32_bulk"))]
+    alone = []
+    for m, kinds in specs:
+        s = solver_mod.Solver(m.desc_ptr)
+        s.set_contraction_kinds(*kinds)
+        s.run(1, 13)
+        alone.append((s.field(), s.traces()))
+        s.close()
+    members = []
+    for m, kinds in specs:
+        s = solver_mod.Solver(m.desc_ptr)
+        s.set_contraction_kinds(*kinds)
+        members.append(s)
+    g = solver_mod.Group(members)
+    g.run(1, 6)
+    g.run(7, 13)
+    for s, (f, t) in zip(members, alone):
+        assert np.array_equal(s.field(), f)
+        assert np.array_equal(s.traces(), t)
+    g.close()
