@@ -544,6 +544,7 @@ def main():
             return ms, ab, ab / (ms * 1e-3) / 1e9, tr
 
         per_launch_ms, abytes, achieved, traffic = kernel_roofline(dom)
+        step_bytes = sum(algorithmic_bytes(mesh, k, prof[k]["elements"]) * nb for k in kinds) * nstage
         per_kernel = {}
         for k in kinds:
             ms_k, ab_k, ach_k, tr_k = kernel_roofline(k)
@@ -576,7 +577,10 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": per_launch_ms,
-                         "per_kernel": per_kernel},
+                         "per_kernel": per_kernel,
+                         # the whole step: all stage launches' algorithmic bytes over the device-timed step
+                         "step_achieved": step_bytes / (dev_ms / steps * 1e-3) / 1e9,
+                         "step_frac": step_bytes / (dev_ms / steps * 1e-3) / 1e9 / peak},
             "kernels": {k: {"launches": prof[k]["launches"], "ms": round(prof[k]["ms"], 3)}
                         for k in ("record", "stage_pml", "stage_main")},
             "per_launch_pass_ms_per_step": prof["span_ms"] / steps,
