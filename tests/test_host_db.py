@@ -154,6 +154,21 @@ def test_unassigned_boundary_raises(tmp_path, built):
         Mesh(d, N=2)
 
 
+def test_source_search_gives_up_like_the_reference(tmp_path, built):
+    """findSource (src/sourceReceiverMod.f90:243-356) starts at the element of
+    the node nearest the source and gives up after 20 rejected elements with
+    "could not find source": at N = 4 a source on a vertical cell edge of a
+    4 x 4 x 2 box, where many tets share the nearest node, is not found. The
+    same point inside a cell of a 5 x 5 x 2 box is."""
+    d = str(tmp_path / "edge")
+    synth.write_twolayer(d, cells=(4, 4, 2), nt=5, nrec=0, src_depth=(900.0, 900.0))
+    with pytest.raises(NexdError, match="could not find source 1 at global coordinates 2000 2000 1100"):
+        Mesh(d, N=4)
+    d = str(tmp_path / "inside")
+    synth.write_twolayer(d, cells=(5, 5, 2), nt=5, nrec=0, src_depth=(900.0, 900.0))
+    assert Mesh(d, N=4).K == 300
+
+
 def test_zener_fit_quality(tmp_path, built):
     """Kaeser et al. (2007) eq. 6: the fitted mechanisms reproduce 1/Q within a
     few percent across the fitted band (src/anelasticMod.f90:59-179)."""
